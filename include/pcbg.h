@@ -1,0 +1,142 @@
+/* pcbg -- C ABI of the B200 search back end for pcbroute.
+ *
+ * Plain pointers and sizes only. Two layers:
+ *   1. pcbg_solve(): one search exactly as pcbroute's gpu_solve() takes it (src/gpu.h:10-57), with the
+ *      GpuQuery vectors flattened into (index, value, count) arrays. gpu_api.cpp implements gpu.h on top of it,
+ *      so a ctypes / cgo / JNI binding sees the same contract as the router does.
+ *   2. pcbg_solve_batch(): many searches whose costs are already resolved in device memory, solved in one
+ *      persistent launch (no counterpart in the reference, which launches ~27 kernels per sweep per search;
+ *      it replaces the per-search sweep loop of src/gpu.cu:493-524 for a whole round of searches).
+ *
+ * Arithmetic contract (shared bit for bit with the CPU oracle):
+ *   - a move into state q in direction m costs W = rint(16 * fl(cf(q) * fac[l][m])) fixed-point units, where
+ *     fac[l][m] = fl(len[m] * dirf[l][m]), len = step (m < 4) or fl(step * sqrt 2) (m >= 4), and fl() is one IEEE
+ *     single-precision multiply; cf >= 1e30 (or a product whose 16x is >= 2^63) is impassable;
+ *   - a via into layer l at cell c costs rint(16 * vcf(c)), vcf = fl(resolved via factor * via_cost);
+ *   - a start costs ceil(16 * g0) (0 if g0 <= 0);
+ *   - distances are exact integer least fixed points; the reported field is d / 16 for every state with
+ *     d <= d(best) (all reached states when no target is reached) and 1e30 elsewhere; best is the target
+ *     state minimising (d, state index).
+ */
+#ifndef PCBG_H
+#define PCBG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PCBG_SCALE 16          /* fixed-point units per length unit of GpuQuery::step */
+#define PCBG_INF_F 1e30f       /* "not reached" / "blocked" as the router reads it */
+
+/* return codes (besides the >= 1 round count of a converged solve) */
+#define PCBG_ERR_FAIL (-1)     /* solve failed: the caller carries on without the GPU (src/gpu.h:55-57) */
+#define PCBG_ERR_BUSY (-3)     /* every slot busy and wait == 0 */
+
+/* A search request. Mirrors GpuQuery (src/gpu.h:10-36); the three std::vector members become index/value/count
+ * triples. All pointers are host pointers borrowed for the duration of the call. */
+typedef struct pcbg_query {
+    int32_t nx, ny, nl;
+    int32_t wi0, wj0, ww, wh;
+    uint16_t me;
+    float via_cost, step;
+    float dirf[8][8];
+    uint8_t lay[8];
+    const float* cst[8];
+    const uint16_t* st[8];
+    const float* vcst;
+    const uint16_t* vst;
+    const uint64_t* tbit;
+    const uint32_t* own_cf_idx;
+    const float* own_cf_val;
+    int64_t n_own_cf;
+    const uint32_t* own_vcf_idx;
+    const float* own_vcf_val;
+    int64_t n_own_vcf;
+    const uint32_t* start_idx;
+    const float* start_val;
+    int64_t n_starts;
+    const uint8_t* prior;
+    int32_t pi0, pj0, pw, ph, pnl;
+    const int32_t* pcol;
+    const int32_t* prow;
+    int32_t play[8];
+    float mlf[256];
+    uint8_t mthr;
+    uint8_t corridor;
+} pcbg_query;
+
+/* The solution of one search. Mirrors GpuOut (src/gpu.h:39-50) plus diagnostics. `d` is a pinned host buffer
+ * owned by the library (nl * rh * rw floats, [l][j][i]); give it back with pcbg_host_release(d, cap). */
+typedef struct pcbg_result {
+    int32_t rx0, ry0, rw, rh, nl, ww, wh;
+    int64_t best;
+    float* d;
+    size_t cap;
+    int32_t rounds;        /* persistent-kernel relaxation rounds of the last rectangle */
+    int32_t tries;         /* rectangles solved (the window grows while a cheaper path may lie outside) */
+    int32_t wide;          /* 1 if 64-bit distances were needed */
+    int64_t tile_visits;   /* tiles relaxed in the last rectangle */
+    double ub;             /* cost of the best target (1e30 if none) */
+} pcbg_result;
+
+/* src/gpu.h:52 (gpu_available): 1 if a device is present and the kernels load. */
+int pcbg_available(void);
+/* src/gpu.h:53-54 (gpu_configure): concurrent solve slots (before first use) and the state cap per solve. */
+void pcbg_configure(int slots, size_t max_states);
+/* src/gpu.h:55-57 (gpu_solve): >= 1 rounds on success, PCBG_ERR_FAIL, or PCBG_ERR_BUSY. Thread-safe. */
+int pcbg_solve(const pcbg_query* q, pcbg_result* out, int wait);
+/* src/gpu.cu:393-407 (GpuOut::reserve / ~GpuOut): pinned output buffers from a pool. */
+float* pcbg_host_acquire(size_t n, size_t* cap);
+void pcbg_host_release(float* p, size_t cap);
+/* Text of the last failure on this thread ("" if none). */
+const char* pcbg_last_error(void);
+
+/* ---- batched device API --------------------------------------------------------------------------------- */
+
+/* One search whose costs are resolved on the device. Device arrays are pitched: state (l, j, i) sits at
+ * (l * hpad + j) * pitch + i, with pitch and hpad multiples of 32 and padding cells impassable (cf >= 1e30,
+ * flags 0, vcf >= 1e30). */
+typedef struct pcbg_search {
+    int32_t rw, rh, nl;
+    int32_t pitch, hpad;
+    float fac[8][8];            /* fl(len[m] * dirf[l][m]) */
+    const float* cf;            /* device [nl][hpad][pitch] resolved step cost factor */
+    const uint8_t* flags;       /* device [nl][hpad][pitch] bit0 via may land, bit1 target */
+    const float* vcf;           /* device [hpad][pitch] resolved via cost, or NULL for no vias */
+    const uint32_t* start_idx;  /* device rect states (l * rh + j) * rw + i */
+    const uint64_t* start_d;    /* device fixed-point start costs */
+    int32_t n_starts;
+    float* out;                 /* device [nl][rh][rw] reported field, or NULL */
+    /* results */
+    int64_t best;               /* rect state of the cheapest target, -1 if none */
+    uint64_t best_d;            /* its fixed-point cost */
+    int32_t status;             /* 0 ok, 1 needed 64-bit distances (solved again wide), < 0 error */
+    int32_t rounds;
+} pcbg_search;
+
+/* Solve n searches in one persistent launch on `stream` (a cudaStream_t, NULL for the legacy stream). Scratch
+ * (distances, tile worklists) comes from the library's device arena. Returns 0 or PCBG_ERR_FAIL. Blocks until
+ * the results are in the structs. */
+int pcbg_solve_batch(pcbg_search* s, int32_t n, void* stream);
+
+/* Tile visits and rounds of the last batch (for throughput accounting). */
+int64_t pcbg_last_batch_tile_visits(void);
+int32_t pcbg_last_batch_rounds(void);
+
+/* ---- seeded synthetic search generator (the batched-search microbenchmark workload) ----------------------- */
+
+/* Fill a pitched search with the seeded workload: per (layer, cell) cost 1 + (h % 16), about 15 % of cells
+ * blocked in value-noise blobs (the same on every layer), via cost `via` per cell, flags, one source and one
+ * target picked among free cells. cf/flags/vcf are the pcbg_search device arrays; src/tgt receive the rect
+ * states chosen (device int64 each). Deterministic in (seed). */
+int pcbg_synth_search(uint64_t seed, int32_t rw, int32_t rh, int32_t nl, int32_t pitch, int32_t hpad, float via,
+                      float* cf, uint8_t* flags, float* vcf, int64_t* src_tgt, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PCBG_H */

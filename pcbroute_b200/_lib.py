@@ -1,0 +1,123 @@
+"""ctypes bindings of the pcbg C ABI (include/pcbg.h) in pcbroute_b200/lib/libpcbgpu.so.
+
+The library is built in-tree (python -m pcbroute_b200.build). There is no fallback: if it is missing, load()
+raises, and every entry point that needs it fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from . import build as _build
+
+LIB_PATH = _build.LIB
+
+# the symbols include/pcbg.h declares (C linkage) and include/gpu.h declares (C++ linkage, mangled)
+PCBG_SYMBOLS = [
+    "pcbg_available", "pcbg_configure", "pcbg_solve", "pcbg_host_acquire", "pcbg_host_release", "pcbg_last_error",
+    "pcbg_solve_batch", "pcbg_last_batch_tile_visits", "pcbg_last_batch_rounds", "pcbg_synth_search",
+]
+GPU_H_SYMBOLS = [
+    "_Z13gpu_availablev",                        # bool gpu_available()
+    "_Z13gpu_configureim",                       # void gpu_configure(int, size_t)
+    "_Z9gpu_solveRK8GpuQueryR6GpuOutb",          # int gpu_solve(const GpuQuery&, GpuOut&, bool)
+    "_ZN6GpuOutD1Ev",                            # GpuOut::~GpuOut()
+    "_ZN6GpuOut7reserveEm",                      # void GpuOut::reserve(size_t)
+    "_ZNK6GpuOutclEl",                           # float GpuOut::operator()(int64_t) const
+]
+
+
+class Query(C.Structure):
+    """struct pcbg_query (GpuQuery of src/gpu.h:10-36 with flattened vectors)."""
+    _fields_ = [
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nl", C.c_int32),
+        ("wi0", C.c_int32), ("wj0", C.c_int32), ("ww", C.c_int32), ("wh", C.c_int32),
+        ("me", C.c_uint16),
+        ("via_cost", C.c_float), ("step", C.c_float),
+        ("dirf", (C.c_float * 8) * 8),
+        ("lay", C.c_uint8 * 8),
+        ("cst", C.c_void_p * 8),
+        ("st", C.c_void_p * 8),
+        ("vcst", C.c_void_p), ("vst", C.c_void_p), ("tbit", C.c_void_p),
+        ("own_cf_idx", C.c_void_p), ("own_cf_val", C.c_void_p), ("n_own_cf", C.c_int64),
+        ("own_vcf_idx", C.c_void_p), ("own_vcf_val", C.c_void_p), ("n_own_vcf", C.c_int64),
+        ("start_idx", C.c_void_p), ("start_val", C.c_void_p), ("n_starts", C.c_int64),
+        ("prior", C.c_void_p),
+        ("pi0", C.c_int32), ("pj0", C.c_int32), ("pw", C.c_int32), ("ph", C.c_int32), ("pnl", C.c_int32),
+        ("pcol", C.c_void_p), ("prow", C.c_void_p),
+        ("play", C.c_int32 * 8),
+        ("mlf", C.c_float * 256),
+        ("mthr", C.c_uint8), ("corridor", C.c_uint8),
+    ]
+
+
+class Result(C.Structure):
+    """struct pcbg_result (GpuOut of src/gpu.h:39-50 plus diagnostics)."""
+    _fields_ = [
+        ("rx0", C.c_int32), ("ry0", C.c_int32), ("rw", C.c_int32), ("rh", C.c_int32), ("nl", C.c_int32),
+        ("ww", C.c_int32), ("wh", C.c_int32),
+        ("best", C.c_int64),
+        ("d", C.POINTER(C.c_float)), ("cap", C.c_size_t),
+        ("rounds", C.c_int32), ("tries", C.c_int32), ("wide", C.c_int32),
+        ("tile_visits", C.c_int64),
+        ("ub", C.c_double),
+    ]
+
+
+class Search(C.Structure):
+    """struct pcbg_search: one device-resident resolved search of a batch."""
+    _fields_ = [
+        ("rw", C.c_int32), ("rh", C.c_int32), ("nl", C.c_int32), ("pitch", C.c_int32), ("hpad", C.c_int32),
+        ("fac", (C.c_float * 8) * 8),
+        ("cf", C.c_void_p), ("flags", C.c_void_p), ("vcf", C.c_void_p),
+        ("start_idx", C.c_void_p), ("start_d", C.c_void_p), ("n_starts", C.c_int32),
+        ("out", C.c_void_p),
+        ("best", C.c_int64), ("best_d", C.c_uint64),
+        ("status", C.c_int32), ("rounds", C.c_int32),
+    ]
+
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load libpcbgpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: run python -m pcbroute_b200.build")
+    lib = C.CDLL(LIB_PATH)
+    lib.pcbg_available.restype = C.c_int
+    lib.pcbg_configure.argtypes = [C.c_int, C.c_size_t]
+    lib.pcbg_solve.argtypes = [C.POINTER(Query), C.POINTER(Result), C.c_int]
+    lib.pcbg_solve.restype = C.c_int
+    lib.pcbg_host_acquire.argtypes = [C.c_size_t, C.POINTER(C.c_size_t)]
+    lib.pcbg_host_acquire.restype = C.POINTER(C.c_float)
+    lib.pcbg_host_release.argtypes = [C.POINTER(C.c_float), C.c_size_t]
+    lib.pcbg_last_error.restype = C.c_char_p
+    lib.pcbg_solve_batch.argtypes = [C.POINTER(Search), C.c_int32, C.c_void_p]
+    lib.pcbg_solve_batch.restype = C.c_int
+    lib.pcbg_last_batch_tile_visits.restype = C.c_int64
+    lib.pcbg_last_batch_rounds.restype = C.c_int32
+    lib.pcbg_synth_search.argtypes = [C.c_uint64, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_float,
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.pcbg_synth_search.restype = C.c_int
+    _lib = lib
+    return lib
+
+
+def exported_symbols() -> list[str]:
+    """Dynamic symbols of the library that include/*.h declare and that are missing (empty: all present)."""
+    lib = load()
+    missing = []
+    for s in PCBG_SYMBOLS + GPU_H_SYMBOLS:
+        try:
+            getattr(lib, s)
+        except AttributeError:
+            missing.append(s)
+    return missing
+
+
+def last_error() -> str:
+    return load().pcbg_last_error().decode()

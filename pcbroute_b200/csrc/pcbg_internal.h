@@ -1,0 +1,81 @@
+// Internal declarations shared by the pcbg engine sources (not part of the C ABI).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "pcbg.h"
+
+namespace pcbg {
+
+// Tile geometry of the relaxation kernel: 32 x 32 cells, every layer of the search (up to 8).
+constexpr int TILE = 32;
+constexpr int MAX_LAYERS = 8;
+
+// Fixed-point limits. INF is a byte pattern so that cudaMemset(0x7F) fills "unreached"; a finite weight is below
+// WLIM so that d + w never wraps (d <= INF, w < 2^31 resp. 2^63) and min(v, d + w) <= v <= INF.
+constexpr uint32_t INF32 = 0x7F7F7F7Fu;
+constexpr uint64_t INF64 = 0x7F7F7F7F7F7F7F7Full;
+constexpr float WLIM32 = 2130706432.0f;               // 2^31 - 2^24
+constexpr float WLIM64 = 4611686018427387904.0f;      // 2^62
+
+// Per-search device descriptor of the relaxation kernel.
+struct SDev {
+    int rw, rh, nl, pitch, hpad, ntx, nty, pad0;
+    float fac[MAX_LAYERS][8];
+    float maxfac[MAX_LAYERS];
+    const float* cf;
+    const uint8_t* fl;
+    const float* vcf;
+    void* dist;
+    uint32_t* stamp;
+    float* out;
+};
+
+// Per-search statistics written by the kernels.
+struct SStat {
+    unsigned long long ub;        // least target distance seen (all ones: none)
+    unsigned long long maxw;      // largest finite weight met in visited tiles
+    unsigned long long best;      // rect state of the cheapest target (all ones: none)
+    unsigned long long maxd;      // largest finite distance in the field
+    unsigned int need_wide;       // a finite weight does not fit 32-bit arithmetic
+    unsigned int pad;
+};
+
+// Search handed to the batch solver (host side).
+struct BatchItem {
+    int rw, rh, nl, pitch, hpad;
+    float fac[MAX_LAYERS][8];
+    const float* cf;
+    const uint8_t* fl;
+    const float* vcf;
+    const uint32_t* start_idx;   // device, rect states
+    const uint64_t* start_d;     // device
+    int n_starts;
+    float* out;
+    // results
+    int64_t best;
+    uint64_t best_d;
+    int status;
+    int rounds;
+};
+
+// Solve a batch on `stream` (blocks until done). Returns 0 or -1 (error text in last_error()).
+int solve_batch(BatchItem* items, int n, cudaStream_t stream);
+
+void set_error(const std::string& s);
+const std::string& last_error();
+
+// Round / tile-visit counters of the last batch on this thread.
+struct BatchStats {
+    int rounds = 0;
+    long long tile_visits = 0;
+};
+BatchStats& last_stats();
+
+inline size_t round_up(size_t x, size_t m) { return (x + m - 1) / m * m; }
+
+}  // namespace pcbg

@@ -1,0 +1,217 @@
+"""Parity of the sm_100a back end with the CPU oracle: bit-exact fields, best targets, rectangles.
+
+Every test here runs the CUDA kernels through the C ABI (libpcbgpu.so) and checks the result against
+oracle/oracle.py on the same seeded inputs.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from pcbroute_b200 import _lib, query, synth
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _torch():
+    import torch
+    assert torch.cuda.is_available()
+    return torch
+
+
+def make_device_search(seed, rw, rh, nl, via):
+    """Generate one microbenchmark search on the device (pitched) and return tensors + numpy copies."""
+    torch = _torch()
+    pitch, hpad = -(-rw // 32) * 32, -(-rh // 32) * 32
+    cf = torch.empty(nl * hpad * pitch, dtype=torch.float32, device="cuda")
+    fl = torch.empty(nl * hpad * pitch, dtype=torch.uint8, device="cuda")
+    vcf = torch.empty(hpad * pitch, dtype=torch.float32, device="cuda")
+    st = torch.empty(2, dtype=torch.int64, device="cuda")
+    rc = _lib.load().pcbg_synth_search(seed, rw, rh, nl, pitch, hpad, via, cf.data_ptr(), fl.data_ptr(),
+                                       vcf.data_ptr(), st.data_ptr(), None)
+    assert rc == 0
+    torch.cuda.synchronize()
+    return dict(rw=rw, rh=rh, nl=nl, pitch=pitch, hpad=hpad, via=via, seed=seed, cf=cf, fl=fl, vcf=vcf, st=st)
+
+
+def dense(t, nl, hpad, pitch, rh, rw):
+    return t.cpu().numpy().reshape(nl, hpad, pitch)[:, :rh, :rw]
+
+
+@pytest.mark.parametrize("rw,rh,nl", [(64, 64, 2), (97, 45, 3), (200, 130, 6), (31, 257, 4), (33, 33, 8)])
+def test_device_generator_matches_numpy(gpu, rw, rh, nl):
+    s = make_device_search(1234 + rw, rw, rh, nl, 17.0)
+    cf, fl, vcf, src, tgt = synth.search_arrays(1234 + rw, rw, rh, nl, 17.0)
+    dcf = dense(s["cf"], nl, s["hpad"], s["pitch"], rh, rw)
+    dfl = dense(s["fl"], nl, s["hpad"], s["pitch"], rh, rw)
+    assert np.array_equal(dcf.view(np.uint32), cf.view(np.uint32))
+    assert np.array_equal(dfl, fl)
+    assert np.array_equal(s["vcf"].cpu().numpy().reshape(s["hpad"], s["pitch"])[:rh, :rw], vcf)
+    assert tuple(s["st"].cpu().tolist()) == (src, tgt)
+    # padding is impassable
+    full = s["cf"].cpu().numpy().reshape(nl, s["hpad"], s["pitch"])
+    assert (full[:, rh:, :] >= 1e30).all() and (full[:, :, rw:] >= 1e30).all()
+
+
+def run_batch(searches, with_out=True):
+    torch = _torch()
+    lib = _lib.load()
+    arr = (_lib.Search * len(searches))()
+    keep = []
+    for k, s in enumerate(searches):
+        a = arr[k]
+        a.rw, a.rh, a.nl, a.pitch, a.hpad = s["rw"], s["rh"], s["nl"], s["pitch"], s["hpad"]
+        fac = synth.microbench_factors(s["nl"])
+        for l in range(8):
+            for m in range(8):
+                a.fac[l][m] = float(fac[l, m])
+        a.cf, a.flags, a.vcf = s["cf"].data_ptr(), s["fl"].data_ptr(), s["vcf"].data_ptr()
+        src = int(s["st"][0].item())
+        si = torch.tensor([max(src, 0)], dtype=torch.int32, device="cuda")
+        sd = torch.zeros(1, dtype=torch.int64, device="cuda")
+        keep += [si, sd]
+        a.start_idx, a.start_d, a.n_starts = si.data_ptr(), sd.data_ptr(), 1 if src >= 0 else 0
+        if with_out:
+            out = torch.empty(s["nl"] * s["rh"] * s["rw"], dtype=torch.float32, device="cuda")
+            keep.append(out)
+            s["out"] = out
+            a.out = out.data_ptr()
+        else:
+            a.out = None
+    rc = lib.pcbg_solve_batch(arr, len(searches), None)
+    assert rc == 0, _lib.last_error()
+    torch.cuda.synchronize()
+    return arr
+
+
+def oracle_of(s):
+    cf, fl, vcf, src, tgt = synth.search_arrays(s["seed"], s["rw"], s["rh"], s["nl"], s["via"])
+    fac = synth.microbench_factors(s["nl"])
+    si = np.array([src] if src >= 0 else [], np.uint32)
+    sd = np.zeros(len(si), np.uint64)
+    dist, best, bd = oracle.dijkstra(fac, cf, fl, vcf, si, sd)
+    return oracle.report(dist, best, bd), best, bd
+
+
+def test_batch_matches_oracle(gpu):
+    rng = np.random.default_rng(5)
+    searches = []
+    for k in range(24):
+        rw, rh = int(rng.integers(20, 320)), int(rng.integers(20, 320))
+        nl = int(rng.integers(2, 7))
+        searches.append(make_device_search(9000 + k, rw, rh, nl, float(rng.integers(8, 33))))
+    arr = run_batch(searches)
+    for k, s in enumerate(searches):
+        field, best, bd = oracle_of(s)
+        assert arr[k].best == best, (k, arr[k].best, best)
+        if best >= 0:
+            assert arr[k].best_d == bd
+        got = s["out"].cpu().numpy().reshape(s["nl"], s["rh"], s["rw"])
+        assert np.array_equal(got.view(np.uint32), field.view(np.uint32)), k
+
+
+def test_batch_without_field_output(gpu):
+    searches = [make_device_search(77 + k, 150 + 13 * k, 90 + 7 * k, 3, 12.0) for k in range(4)]
+    arr = run_batch(searches, with_out=False)
+    for k, s in enumerate(searches):
+        _, best, bd = oracle_of(s)
+        assert (arr[k].best, arr[k].best_d if best >= 0 else 0) == (best, bd if best >= 0 else 0)
+
+
+def _cmp_query(q):
+    out = query.GpuOut()
+    rc = query.gpu_solve(q, out)
+    orc, ref = oracle.solve(q)
+    if orc < 0:
+        assert rc == -1
+        return out, ref
+    assert rc >= 1, _lib.last_error()
+    assert (out.rx0, out.ry0, out.rw, out.rh, out.NL, out.ww, out.wh) == \
+        (ref.rx0, ref.ry0, ref.rw, ref.rh, ref.NL, ref.ww, ref.wh)
+    assert out.best == ref.best
+    assert out.tries == ref.tries
+    assert np.array_equal(out.d.view(np.uint32), ref.d.view(np.uint32))
+    return out, ref
+
+
+@pytest.mark.parametrize("seed", range(6))
+@pytest.mark.parametrize("opts", [
+    dict(),
+    dict(prior=True),
+    dict(prior=True, corridor=True),
+    dict(vias=False),
+    dict(unusable_layer=True),
+    dict(own=False, n_starts=1, n_targets=1),
+])
+def test_query_matches_oracle(gpu, seed, opts):
+    q = synth.random_query(100 + seed, nx=120, ny=100, nl=3 + seed % 3, **opts)
+    _cmp_query(q)
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_query_rectangle_growth(gpu, seed):
+    """Windows much larger than the start/target box: the solved rectangle grows by 80 x 3^k cells."""
+    rng = np.random.default_rng(seed)
+    q = synth.random_query(300 + seed, nx=900, ny=700, nl=2, window=(10, 20, 880, 670), n_starts=1, n_targets=2)
+    # put the starts and targets close together so the first rectangle is small
+    fwn = q.ww * q.wh
+    cx, cy = int(rng.integers(200, 600)), int(rng.integers(150, 450))
+    q.starts = [((cy * q.ww + cx), 0.0)]
+    q.tbit[:] = 0
+    for dx, dy in [(int(rng.integers(5, 60)), int(rng.integers(-40, 40))), (-30, 25)]:
+        t = (cy + dy) * q.ww + cx + dx + fwn * int(rng.integers(0, 2))
+        q.tbit[t >> 6] |= np.uint64(1) << np.uint64(t & 63)
+    out, ref = _cmp_query(q)
+    assert ref.rw < q.ww or ref.rh < q.wh  # a proper sub-rectangle was enough
+
+
+def test_unreachable_target(gpu):
+    q = synth.random_query(7, nx=80, ny=60, nl=2, n_starts=1, n_targets=1, vias=False, own=False)
+    fwn = q.ww * q.wh
+    # wall the target in on both layers (blocked ring)
+    t = (q.wh // 2) * q.ww + q.ww // 2
+    q.tbit[:] = 0
+    q.tbit[t >> 6] |= np.uint64(1) << np.uint64(t & 63)
+    for l in range(2):
+        for dj in range(-2, 3):
+            for di in range(-2, 3):
+                if max(abs(di), abs(dj)) == 2:
+                    c = (q.wj0 + q.wh // 2 + dj) * q.nx + q.wi0 + q.ww // 2 + di
+                    q.cst[l, c] = 1e30
+    q.starts = [(0 * fwn + 3 * q.ww + 3, 0.0)]
+    out, ref = _cmp_query(q)
+    assert out.best == -1 and ref.best == -1
+
+
+def test_start_on_target(gpu):
+    q = synth.random_query(8, nx=70, ny=50, nl=2, n_starts=1, n_targets=1, own=False)
+    q.tbit[:] = 0
+    s = q.starts[0][0]
+    q.tbit[s >> 6] |= np.uint64(1) << np.uint64(s & 63)
+    out, ref = _cmp_query(q)
+    assert out.best == s
+
+
+@pytest.mark.parametrize("ww,wh,nl", [(1, 1, 2), (33, 1, 1), (1, 65, 3), (45, 37, 8)])
+def test_odd_windows(gpu, ww, wh, nl):
+    q = synth.random_query(9 + ww + wh, nx=ww + 10, ny=wh + 10, nl=nl, window=(5, 5, ww, wh), n_starts=1,
+                           n_targets=1, own=False)
+    _cmp_query(q)
+
+
+def test_wide_distances(gpu):
+    """A target reachable only across very expensive cells: 32-bit weights overflow, the 64-bit pass takes over."""
+    q = synth.random_query(21, nx=100, ny=40, nl=1, window=(0, 0, 100, 40), n_starts=1, n_targets=1, vias=False,
+                           own=False)
+    q.cst[:] = np.abs(q.cst[:]).clip(1, 4).astype(np.float32)
+    q.st[:] = 0
+    # a wall at x = 50 of cost 5e6 (16 * 70 * 5e6 > 2^31)
+    for j in range(40):
+        q.cst[0, j * 100 + 50] = np.float32(5e6)
+    q.starts = [(20 * 100 + 10, 0.0)]
+    q.tbit[:] = 0
+    t = 20 * 100 + 90
+    q.tbit[t >> 6] |= np.uint64(1) << np.uint64(t & 63)
+    out, ref = _cmp_query(q)
+    assert out.wide and out.best == t and ref.ub > 5e6
