@@ -1,0 +1,396 @@
+"""Benchmark of the B200 search back end: the batched-search microbenchmark workload.
+
+Workload (seeded, synthetic): 4096 independent single-source single-target searches; window sides log-uniform in
+[64, 2048) cells, 2-6 layers, per-(layer, cell) cost 1-16, ~15 % of cells blocked in value-noise blobs, via cost
+8-32; about 5.4e9 states in all. They are solved in waves of 512 searches: one step = one wave, solved in one
+persistent launch (pcbg_solve_batch). The workload cycles through the 8 waves.
+
+Metric: Gcell-relax/s = 9 x (states of the windows solved) / time. A state has 9 incoming moves (8 in-layer
+moves and a via); an exact single-source solve must relax every one of them at least once, so this counts the
+problem solved, not the work an algorithm spends on it, and is the same number for the GPU tile solver and a CPU
+Dijkstra.
+
+  python bench.py [--gpus N --steps K --warmup W]      # this back end (one JSON line on rank 0)
+  python bench.py --impl reference ...                  # the CPU arm (exact Dijkstra on all host cores)
+
+Multi-GPU: one process per GPU (torchrun); each rank solves its own waves (no collective on the data path, weak
+scaling); the step time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "route s to byte-identical SES: plain GPU vs learned-batched GPU; Gcell-relax/s"
+UNIT = "Gcell-relax/s"
+SEED = 20261203
+WORKLOAD = ("batched-search microbenchmark: 4096 seeded single-source single-target searches, windows log-uniform "
+            "64-2048 cells per side, 2-6 layers, cost 1-16 per cell, 15% blocked in value-noise blobs, via cost "
+            "8-32; one step = one wave of 512 searches in one persistent launch")
+BYTES_PER_LAYER_VISIT = 32 * 32 * 13     # per staged layer of a tile: cf 4 + flags 1 + distance read 4 + write 4
+BYTES_PER_TILE_VISIT = 32 * 32 * 4       # per tile: via cost of each cell
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ------------------------------------------------------------------------------------------------- CPU baseline
+
+def cpu_solve_sample(sizes, budget_s: float, threads: int, max_searches: int):
+    """Solve searches of the workload in order on the host (exact Dijkstra, `threads` threads) until budget_s of
+    work or max_searches. Returns (states, seconds, searches)."""
+    from oracle import oracle
+    from pcbroute_b200 import _lib, synth
+    lib = _lib.load()
+    done_states, secs, n = 0, 0.0, 0
+    chunk = max(threads, 8)
+    k = 0
+    while k < min(len(sizes), max_searches) and secs < budget_s:
+        batch = []
+        for (rw, rh, nl, via, sseed) in sizes[k:k + chunk]:
+            cf = np.empty((nl, rh, rw), np.float32)
+            fl = np.empty((nl, rh, rw), np.uint8)
+            vcf = np.empty((rh, rw), np.float32)
+            st = np.empty(2, np.int64)
+            lib.pcbg_synth_search_host(sseed, rw, rh, nl, via, cf.ctypes.data, fl.ctypes.data, vcf.ctypes.data,
+                                       st.ctypes.data, threads)
+            src = int(st[0])
+            batch.append(dict(fac=synth.microbench_factors(nl), cf=cf, flags=fl, vcf=vcf,
+                              start_idx=np.array([src] if src >= 0 else [], np.uint32),
+                              start_d=np.zeros(1 if src >= 0 else 0, np.uint64), states=rw * rh * nl))
+        t0 = time.perf_counter()
+        oracle.solve_many(batch, threads)
+        secs += time.perf_counter() - t0
+        done_states += sum(b["states"] for b in batch)
+        n += len(batch)
+        k += chunk
+    return done_states, secs, n
+
+
+def run_reference(args):
+    ws, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    from pcbroute_b200 import synth
+    threads = os.cpu_count() or 1
+    sizes = synth.microbench_sizes(SEED, args.searches)
+    # calibrate the per-step sample so that the whole run stays within a few minutes
+    st, secs, n = cpu_solve_sample(sizes, 4.0, threads, args.wave)
+    per_step = max(threads, n)
+    for _ in range(max(0, args.warmup - 1)):
+        cpu_solve_sample(sizes, 1e9, threads, per_step)
+    tot_states, tot_s = 0, 0.0
+    for _ in range(args.steps):
+        s, t, _n = cpu_solve_sample(sizes, 1e9, threads, per_step)
+        tot_states += s
+        tot_s += t
+    v = 9.0 * tot_states / tot_s / 1e9
+    sample = (f"first {per_step} searches of the workload ({tot_states // max(1, args.steps)} states) per step, "
+              f"exact Dijkstra (oracle/pcb_oracle.c) on {threads} host threads")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(1e3 * tot_s / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "searches": args.searches, "wave": args.wave, "seed": SEED,
+                   "parallelism": f"{threads} host threads"},
+        "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------------------------------------- GPU arm
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--searches", type=int, default=4096)
+    ap.add_argument("--wave", type=int, default=512)
+    ap.add_argument("--e2e-waves", type=int, default=2)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from pcbroute_b200 import _lib, synth
+
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    lib = _lib.load()
+    if not lib.pcbg_available():
+        raise RuntimeError("B200 back end unavailable: " + _lib.last_error())
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+
+    sizes = synth.microbench_sizes(SEED, args.searches)
+    waves = [sizes[i:i + args.wave] for i in range(0, len(sizes), args.wave)]
+    nw = len(waves)
+    my = [waves[(rank + ws * k) % nw] for k in range(max(1, -(-nw // ws)))]
+
+    # generate every search of my waves on the device (pitched layout), once
+    def make(sz):
+        rw, rh, nl, via, sseed = sz
+        pitch, hpad = -(-rw // 32) * 32, -(-rh // 32) * 32
+        cf = torch.empty(nl * hpad * pitch, dtype=torch.float32, device="cuda")
+        fl = torch.empty(nl * hpad * pitch, dtype=torch.uint8, device="cuda")
+        vcf = torch.empty(hpad * pitch, dtype=torch.float32, device="cuda")
+        st = torch.empty(2, dtype=torch.int64, device="cuda")
+        assert lib.pcbg_synth_search(sseed, rw, rh, nl, pitch, hpad, via, cf.data_ptr(), fl.data_ptr(),
+                                     vcf.data_ptr(), st.data_ptr(), sp) == 0
+        return dict(rw=rw, rh=rh, nl=nl, pitch=pitch, hpad=hpad, cf=cf, fl=fl, vcf=vcf, st=st)
+
+    dev_waves = [[make(sz) for sz in w] for w in my]
+    torch.cuda.synchronize()
+
+    def search_array(wave, outs=None):
+        arr = (_lib.Search * len(wave))()
+        keep = []
+        for k, s in enumerate(wave):
+            a = arr[k]
+            a.rw, a.rh, a.nl, a.pitch, a.hpad = s["rw"], s["rh"], s["nl"], s["pitch"], s["hpad"]
+            fac = synth.microbench_factors(s["nl"])
+            for l in range(8):
+                for m in range(8):
+                    a.fac[l][m] = float(fac[l, m])
+            a.cf, a.flags, a.vcf = s["cf"].data_ptr(), s["fl"].data_ptr(), s["vcf"].data_ptr()
+            si = s["st"][:1].to(torch.int32).clamp_(min=0)
+            sd = torch.zeros(1, dtype=torch.int64, device="cuda")
+            keep += [si, sd]
+            a.start_idx, a.start_d = si.data_ptr(), sd.data_ptr()
+            a.n_starts = 1
+            a.out = outs[k].data_ptr() if outs is not None else None
+        return arr, keep
+
+    # searches whose source could not be placed are dropped from the wave (none are expected)
+    arrays = [search_array(w) for w in dev_waves]
+    states = [sum(s["rw"] * s["rh"] * s["nl"] for s in w) for w in dev_waves]
+
+    iters = [0]
+
+    def solve(k):
+        arr, _ = arrays[k % len(arrays)]
+        rc = lib.pcbg_solve_batch(arr, len(arr), sp)
+        if rc != 0:
+            raise RuntimeError("pcbg_solve_batch failed: " + _lib.last_error())
+        iters[0] += lib.pcbg_last_batch_local_iters()
+        return (lib.pcbg_last_batch_kernel_ms(), lib.pcbg_last_batch_tile_visits(), lib.pcbg_last_batch_layer_visits(),
+                lib.pcbg_last_batch_launches(), lib.pcbg_last_batch_rounds())
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+
+    for k in range(args.warmup):
+        solve(k)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    kms, tv, lv, launches, rounds, st_done = 0.0, 0, 0, 0, 0, 0
+    iters[0] = 0
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for k in range(args.steps):
+            a, b, c, d, r = solve(k)
+            kms += a
+            tv += b
+            lv += c
+            launches += d
+            rounds += r
+            st_done += states[k % len(states)]
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    tot = torch.tensor([float(st_done)], dtype=torch.float64, device="cuda")
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+    ms_max, states_all = float(t.item()), float(tot.item())
+    value = 9.0 * states_all / (ms_max / 1e3) / 1e9
+    alg_bytes = lv * BYTES_PER_LAYER_VISIT + tv * BYTES_PER_TILE_VISIT
+    peak, peak_kind = peaks()
+    achieved = alg_bytes / (kms / 1e3) / 1e9 if kms > 0 else 0.0
+
+    # ---- end to end: host (pinned) inputs -> device, solve, reported fields -> host, every step
+    e2e = None
+    if not args.no_e2e:
+        ew = dev_waves[:max(1, min(args.e2e_waves, len(dev_waves)))]
+        host_in, outs_d, outs_h, e_arrays = [], [], [], []
+        for w in ew:
+            hi = [(s["cf"].cpu().pin_memory(), s["fl"].cpu().pin_memory(), s["vcf"].cpu().pin_memory()) for s in w]
+            od = [torch.empty(s["rw"] * s["rh"] * s["nl"], dtype=torch.float32, device="cuda") for s in w]
+            oh = [torch.empty(s["rw"] * s["rh"] * s["nl"], dtype=torch.float32).pin_memory() for s in w]
+            host_in.append(hi)
+            outs_d.append(od)
+            outs_h.append(oh)
+            e_arrays.append(search_array(w, od))
+        h2d = [sum(x.numel() * x.element_size() for trip in hi for x in trip) for hi in host_in]
+        d2h = [sum(x.numel() * 4 for x in oh) for oh in outs_h]
+        e_states = [sum(s["rw"] * s["rh"] * s["nl"] for s in w) for w in ew]
+
+        def e2e_step(k):
+            i = k % len(ew)
+            for s, (hc, hf, hv) in zip(ew[i], host_in[i]):
+                s["cf"].copy_(hc, non_blocking=True)
+                s["fl"].copy_(hf, non_blocking=True)
+                s["vcf"].copy_(hv, non_blocking=True)
+            arr, _ = e_arrays[i]
+            if lib.pcbg_solve_batch(arr, len(arr), sp) != 0:
+                raise RuntimeError("pcbg_solve_batch failed: " + _lib.last_error())
+            for od, oh in zip(outs_d[i], outs_h[i]):
+                oh.copy_(od, non_blocking=True)
+            return e_states[i], h2d[i], d2h[i], lib.pcbg_last_batch_launches()
+
+        for k in range(min(args.warmup, 2)):
+            e2e_step(k)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        es, eb_in, eb_out = 0, 0, 0
+        f0.record(stream)
+        for k in range(args.steps):
+            a, b, c, _ = e2e_step(k)
+            es += a
+            eb_in += b
+            eb_out += c
+        f1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        et = torch.tensor([f0.elapsed_time(f1)], dtype=torch.float64, device="cuda")
+        etot = torch.tensor([float(es)], dtype=torch.float64, device="cuda")
+        if ws > 1:
+            dist.all_reduce(et, op=dist.ReduceOp.MAX)
+            dist.all_reduce(etot, op=dist.ReduceOp.SUM)
+        e2e = {"value": round(9.0 * float(etot.item()) / (float(et.item()) / 1e3) / 1e9, 4), "unit": UNIT,
+               "h2d_bytes_per_step": int(eb_in // args.steps), "d2h_bytes_per_step": int(eb_out // args.steps),
+               "waves": len(ew), "api": "pcbg_solve_batch from pinned host buffers, reported fields read back"}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        cst, csecs, cn = cpu_solve_sample(sizes, args.cpu_budget, threads, args.wave)
+        cv = 9.0 * cst / csecs / 1e9
+        cpu = {"value": round(cv, 4), "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"first {cn} searches of the workload ({cst} states), exact Dijkstra "
+                         f"(oracle/pcb_oracle.c) on {threads} host threads, {csecs:.1f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "searches": args.searches, "wave": args.wave, "seed": SEED,
+                       "states_per_step": int(states_all / args.steps), "parallelism": f"replicas x{ws}",
+                       "l2": "inputs larger than L2 (several GB per wave)",
+                       "tile_visits_per_step": tv // args.steps, "rounds_per_step": rounds // args.steps,
+                       "state_visits_per_state": round(lv * 1024 / max(1, st_done), 3),
+                       "local_iters_per_visit": round(iters[0] / max(1, tv), 3)},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": None,
+                         "kernel": "relax_kernel (persistent tile relaxation)",
+                         "kernel_ms_per_step": round(kms / args.steps, 3), "peak_kind": peak_kind},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -122,9 +122,15 @@ typedef struct pcbg_search {
  * the results are in the structs. */
 int pcbg_solve_batch(pcbg_search* s, int32_t n, void* stream);
 
-/* Tile visits and rounds of the last batch (for throughput accounting). */
+/* Counters of the last batch solved on this thread (for throughput and roofline accounting): tile visits, the sum
+ * over visits of the search's layer count (each layer of a visit stages 32 x 32 states), relaxation rounds, the
+ * device time of the relaxation launches in ms (CUDA events on the launch stream), and kernels launched. */
 int64_t pcbg_last_batch_tile_visits(void);
+int64_t pcbg_last_batch_layer_visits(void);
 int32_t pcbg_last_batch_rounds(void);
+float pcbg_last_batch_kernel_ms(void);
+int32_t pcbg_last_batch_launches(void);
+int64_t pcbg_last_batch_local_iters(void);   /* sum over tile visits of local relaxation iterations */
 
 /* ---- seeded synthetic search generator (the batched-search microbenchmark workload) ----------------------- */
 
@@ -134,6 +140,9 @@ int32_t pcbg_last_batch_rounds(void);
  * states chosen (device int64 each). Deterministic in (seed). */
 int pcbg_synth_search(uint64_t seed, int32_t rw, int32_t rh, int32_t nl, int32_t pitch, int32_t hpad, float via,
                       float* cf, uint8_t* flags, float* vcf, int64_t* src_tgt, void* stream);
+/* The same search into dense host arrays (cf/flags [nl][rh][rw], vcf [rh][rw]) on `threads` host threads. */
+int pcbg_synth_search_host(uint64_t seed, int32_t rw, int32_t rh, int32_t nl, float via, float* cf, uint8_t* flags,
+                           float* vcf, int64_t* src_tgt, int32_t threads);
 
 #ifdef __cplusplus
 }

@@ -23,8 +23,13 @@ constexpr float WLIM32 = 2130706432.0f;               // 2^31 - 2^24
 constexpr float WLIM64 = 4611686018427387904.0f;      // 2^62
 
 // Per-search device descriptor of the relaxation kernel.
+//   mode 1 (joint): the moves of a layer fall into weight classes x (moves 0, 1), y (2, 3), diagonal (4-7) with
+//     one factor each; a visit stages one integer weight plane per class (K = 2 when x and y share a factor on
+//     every layer, else 3: plane_h / plane_v / plane_d) and relaxes all layers of a line jointly.
+//   mode 0 (general): any per-move factors and 64-bit distances; per-layer scans with weights computed per move.
 struct SDev {
-    int rw, rh, nl, pitch, hpad, ntx, nty, pad0;
+    int rw, rh, nl, pitch, hpad, ntx, nty, mode;
+    int K, plane_h, plane_v, plane_d;
     float fac[MAX_LAYERS][8];
     float maxfac[MAX_LAYERS];
     const float* cf;
@@ -72,7 +77,11 @@ const std::string& last_error();
 // Round / tile-visit counters of the last batch on this thread.
 struct BatchStats {
     int rounds = 0;
-    long long tile_visits = 0;
+    long long tile_visits = 0;     // tile visits (each stages and relaxes every layer of a 32 x 32 tile)
+    long long layer_visits = 0;    // sum over visits of the search's layer count
+    float kernel_ms = 0.f;         // device time of the relaxation launches (CUDA events on the launch stream)
+    int launches = 0;              // kernels this library launched for the batch
+    long long local_iters = 0;     // sum over tile visits of the local relaxation iterations
 };
 BatchStats& last_stats();
 

@@ -2,21 +2,26 @@
 //
 // The reference (src/gpu.cu:122-363, 488-524) relaxes a search window with 8 directional min-plus sweeps plus a
 // via pass, 27 launches and one host sync per sweep, until nothing changes. Here the same relaxation rule
-// (move into a state costs its factor times the move's length and direction factor, vias land only where a via
+// (a move into a state costs its factor times the move's length and direction factor; vias land only where a via
 // may, src/gpu.cu:154-155, 332-350) is solved to its exact integer least fixed point by a tiled worklist:
 //
 //   * the window is cut into 32 x 32-cell tiles holding every layer; a tile visit stages the tile's distances
-//     (with a one-cell halo from its neighbours), cost factors, via costs and via/target masks in shared memory
-//     and relaxes them to a local fixed point (directional line scans +x/-x, +y/-y, both diagonals, vias);
-//   * a tile whose edge cells improved (to a cost not above the best target found so far) queues the neighbours
-//     that read those cells for the next round;
-//   * one persistent cooperative launch runs all rounds of all searches of a batch, with a bounded software
-//     grid barrier between rounds, so a whole round of searches with uneven windows shares the GPU.
+//     (with a one-cell halo from its neighbours), integer move weights, via weights and via/target masks in shared
+//     memory and relaxes them to a local fixed point;
+//   * the local relaxation scans lines (rows, columns, both diagonals, each way) with all layers of a line in one
+//     thread, mixing vias at every cell of the line, so a path that changes layers along a straight run settles in
+//     one pass; the four line families run at once on separate warps, with shared-memory atomicMin updates so that
+//     every stored value only decreases;
+//   * a tile whose edge cell improved below the staged value of an adjacent cell of a neighbour (and not above the
+//     best target found so far) queues that neighbour for the next round;
+//   * one persistent cooperative launch runs all rounds of all searches of a batch, with a bounded software grid
+//     barrier between rounds, so a whole round of searches with uneven windows and layer counts shares the GPU.
 //
-// Exactness: distances are fixed-point integers (pcbg.h), min-plus over integers is exact and associative, so
-// the least fixed point is unique and independent of the tile order; every state whose least cost is at most the
-// best target's is exact (the dirty rule only drops improvements above the best target, which cannot lie on a
-// path that matters), and the epilogue reports exactly those.
+// Exactness: distances are fixed-point integers (pcbg.h); min-plus over integers is exact and associative, so the
+// least fixed point is unique and any monotone schedule reaches it. A visit ends only after a full pass changed
+// nothing, and a neighbour is skipped only when no edge value can lower its adjacent cells; improvements above the
+// best target are not propagated (no path through them can matter). The epilogue reports every state at or below
+// the best target's cost, and those are exact.
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -29,15 +34,17 @@ namespace pcbg {
 
 namespace {
 
-constexpr int NT = 256;                 // threads per tile block
+constexpr int NT = 192;                 // threads per tile block: 6 warps, one per line family and direction pair
 constexpr int HS = TILE + 2;            // tile side with halo
-constexpr int DSTR = TILE + 3;          // shared row stride of distances (odd: conflict-free row and column scans)
-constexpr int CSTR = TILE + 1;          // shared row stride of cost factors / per-cell arrays
+constexpr int DSTR = TILE + 3;          // shared row stride of distances (odd: conflict-free row, column, diagonal)
+constexpr int CSTR = TILE + 1;          // shared row stride of per-state and per-cell arrays
+constexpr int LS = HS * DSTR;           // distance plane stride (one layer)
+constexpr int WLS = TILE * CSTR;        // weight plane stride (one layer)
 constexpr int MAX_IT = 64;              // local iterations before a tile is re-queued instead
 constexpr long long BAR_SPIN_LIMIT = 1ll << 24;   // polls (with __nanosleep) before a barrier wait gives up
 
 // control words of a batch
-enum { C_CNT = 0, C_NEXT = 3, C_BAR = 6, C_GEN = 7, C_ERR = 8, C_ROUNDS = 9, C_OVF = 10, C_N = 16 };
+enum { C_CNT = 0, C_NEXT = 3, C_BAR = 6, C_GEN = 7, C_ERR = 8, C_ROUNDS = 9, C_N = 16 };
 enum { ERR_BARRIER = 1, ERR_ROUNDS = 2, ERR_OVERFLOW = 4 };
 
 template <typename DT> struct Lim;
@@ -71,26 +78,34 @@ struct SolveArgs {
     SStat* st;
     int n;
     int nlmax;
+    int kmax;                     // weight planes of joint-mode searches (0: none in the batch)
     unsigned long long* wl;       // 3 rotating worklists of `cap` items: (search << 32) | tile
     unsigned int cap;
     unsigned int* ctl;
-    unsigned long long* visits;
+    unsigned long long* visits;   // tile visits, layer visits, local iterations
     int max_rounds;
 };
 
-struct SmemLayout {
-    size_t d, c, w, e, m, total;
+// Shared memory of a visit. d: distances with halo [nl][HS][DSTR]; w: joint mode, K integer weight planes
+// [K][nl][TILE][CSTR] (general mode: float cost factors [nl][TILE][CSTR]); v: via weight per cell; e: staged edge
+// values [nl][4][TILE]; m: via-landing and target layer masks per cell (u32).
+struct Lay {
+    size_t d, w, v, e, m, total;
 };
-__host__ __device__ inline SmemLayout smem_layout(int nlm, size_t dsz) {
-    SmemLayout L;
+__host__ __device__ inline Lay layout(int nlm, int planes, size_t dsz) {
+    Lay L;
     size_t o = 0;
-    L.d = o; o += size_t(nlm) * HS * DSTR * dsz; o = (o + 15) & ~size_t(15);
-    L.c = o; o += size_t(nlm) * TILE * CSTR * 4; o = (o + 15) & ~size_t(15);
-    L.w = o; o += size_t(TILE) * CSTR * dsz; o = (o + 15) & ~size_t(15);
+    L.d = o; o += size_t(nlm) * LS * dsz; o = (o + 15) & ~size_t(15);
+    L.w = o; o += size_t(planes) * nlm * WLS * 4; o = (o + 15) & ~size_t(15);
+    L.v = o; o += size_t(WLS) * dsz; o = (o + 15) & ~size_t(15);
     L.e = o; o += size_t(nlm) * 4 * TILE * dsz; o = (o + 15) & ~size_t(15);
-    L.m = o; o += size_t(2) * TILE * CSTR; o = (o + 15) & ~size_t(15);
+    L.m = o; o += size_t(2) * WLS * 4; o = (o + 15) & ~size_t(15);
     L.total = o;
     return L;
+}
+__host__ __device__ inline Lay layout_for(int nlm, int kmax, size_t dsz, int mode) {
+    // one dynamic allocation serves both modes: the larger of the two layouts, same offsets per mode
+    return mode ? layout(nlm, kmax, 4) : layout(nlm, 1, dsz);
 }
 
 // Software grid barrier with a bounded wait: every block of the cooperative launch is resident, so the wait ends
@@ -127,7 +142,277 @@ __device__ __forceinline__ void enqueue(const SolveArgs& a, const SDev& S, int s
     else atomicOr(a.ctl + C_ERR, unsigned(ERR_OVERFLOW));
 }
 
-// One tile visit: stage, relax to a local fixed point, write back, queue neighbours, report targets.
+struct VisitShared {
+    unsigned int marks, any, wide, iters;
+    unsigned long long tmin, wmax;
+};
+
+// ---- staging shared by both modes ----
+
+template <typename DT>
+__device__ void stage_dist(const SDev& S, DT* dS, int x0, int y0) {
+    const DT* dist = reinterpret_cast<const DT*>(S.dist);
+    for (int idx = threadIdx.x; idx < S.nl * HS * HS; idx += NT) {
+        const int l = idx / (HS * HS), rem = idx % (HS * HS), r = rem / HS, c = rem % HS;
+        const int gy = y0 + r - 1, gx = x0 + c - 1;
+        DT v = Lim<DT>::INF;
+        if (gy >= 0 && gy < S.hpad && gx >= 0 && gx < S.pitch) v = dist[(size_t(l) * S.hpad + gy) * S.pitch + gx];
+        dS[l * LS + r * DSTR + c] = v;
+    }
+}
+
+// via weight per cell and the via-landing / target layer masks
+template <typename DT>
+__device__ void stage_cells(const SDev& S, DT* vS, uint32_t* vokS, uint32_t* tgS, int x0, int y0, bool& wide,
+                            unsigned long long& wmax) {
+    for (int cell = threadIdx.x; cell < TILE * TILE; cell += NT) {
+        const int r = cell >> 5, c = cell & 31;
+        DT wv = Lim<DT>::INF;
+        if (S.vcf) {
+            const float v = S.vcf[size_t(y0 + r) * S.pitch + x0 + c];
+            if (v < 1e30f) {
+                const float y = __fmul_rn(v, 16.0f);
+                if (!(y < Lim<DT>::wlim())) wide = true;
+                else { wv = qweight<DT>(v, 1.0f); wmax = max(wmax, static_cast<unsigned long long>(wv)); }
+            }
+        }
+        vS[r * CSTR + c] = wv;
+        unsigned int vm = 0, tm = 0;
+        for (int l = 0; l < S.nl; ++l) {
+            const uint8_t f = S.fl[(size_t(l) * S.hpad + y0 + r) * S.pitch + x0 + c];
+            vm |= unsigned(f & 1) << l;
+            tm |= unsigned((f >> 1) & 1) << l;
+        }
+        vokS[r * CSTR + c] = vm;
+        tgS[r * CSTR + c] = tm;
+    }
+}
+
+// edge cell k of side (0 left, 1 right, 2 top, 3 bottom) in tile coordinates
+__device__ __forceinline__ void edge_rc(int side, int k, int& r, int& c) {
+    r = side <= 1 ? k : (side == 2 ? 0 : TILE - 1);
+    c = side == 0 ? 0 : (side == 1 ? TILE - 1 : k);
+}
+
+template <typename DT>
+__device__ void save_edges(const SDev& S, const DT* dS, DT* eS) {
+    for (int idx = threadIdx.x; idx < S.nl * 4 * TILE; idx += NT) {
+        const int l = idx / (4 * TILE), side = (idx / TILE) & 3, k = idx % TILE;
+        int r, c;
+        edge_rc(side, k, r, c);
+        eS[idx] = dS[l * LS + (r + 1) * DSTR + c + 1];
+    }
+}
+
+// ---- joint-layer line scans (mode 1) ----
+
+// One cell of a line: every layer's move from the previous cell of the line, then vias among the layers.
+template <int NL>
+__device__ __forceinline__ void jstep(uint32_t* dS, const uint32_t* wP, const uint32_t* vS, const uint32_t* vokS,
+                                      int dofs, int wofs, uint32_t (&prev)[NL], int& ch) {
+    uint32_t v[NL], c[NL];
+    uint32_t m = INF32;
+    #pragma unroll
+    for (int l = 0; l < NL; ++l) {
+        v[l] = dS[l * LS + dofs];
+        c[l] = min(v[l], prev[l] + wP[l * WLS + wofs]);
+        m = min(m, c[l]);
+    }
+    const uint32_t mv = m + vS[wofs];
+    const uint32_t vm = vokS[wofs];
+    #pragma unroll
+    for (int l = 0; l < NL; ++l) {
+        if ((vm >> l) & 1u) c[l] = min(c[l], mv);
+        if (c[l] < v[l]) { atomicMin(dS + l * LS + dofs, c[l]); ch = 1; }
+        prev[l] = c[l];
+    }
+}
+
+template <int NL>
+__device__ int joint_pass(const SDev& S, uint32_t* dS, const uint32_t* wS, const uint32_t* vS, const uint32_t* vokS) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int ch = 0;
+    uint32_t prev[NL];
+    if (warp == 0) {            // rows: +x then -x
+        const uint32_t* wP = wS + S.plane_h * S.nl * WLS;
+        const int r = lane;
+        #pragma unroll
+        for (int l = 0; l < NL; ++l) prev[l] = dS[l * LS + (r + 1) * DSTR];
+        for (int k = 0; k < TILE; ++k) jstep<NL>(dS, wP, vS, vokS, (r + 1) * DSTR + k + 1, r * CSTR + k, prev, ch);
+        #pragma unroll
+        for (int l = 0; l < NL; ++l) prev[l] = dS[l * LS + (r + 1) * DSTR + TILE + 1];
+        for (int k = TILE - 1; k >= 0; --k) jstep<NL>(dS, wP, vS, vokS, (r + 1) * DSTR + k + 1, r * CSTR + k, prev, ch);
+    } else if (warp == 1) {     // columns: +y then -y
+        const uint32_t* wP = wS + S.plane_v * S.nl * WLS;
+        const int c = lane;
+        #pragma unroll
+        for (int l = 0; l < NL; ++l) prev[l] = dS[l * LS + c + 1];
+        for (int k = 0; k < TILE; ++k) jstep<NL>(dS, wP, vS, vokS, (k + 1) * DSTR + c + 1, k * CSTR + c, prev, ch);
+        #pragma unroll
+        for (int l = 0; l < NL; ++l) prev[l] = dS[l * LS + (TILE + 1) * DSTR + c + 1];
+        for (int k = TILE - 1; k >= 0; --k) jstep<NL>(dS, wP, vS, vokS, (k + 1) * DSTR + c + 1, k * CSTR + c, prev, ch);
+    } else if (warp < 4) {      // main diagonals i - j = e: (+,+) then (-,-)
+        const int e = (warp - 2) * 32 + lane - (TILE - 1);
+        if (e <= TILE - 1) {
+            const uint32_t* wP = wS + S.plane_d * S.nl * WLS;
+            const int i0 = e > 0 ? e : 0, j0 = e < 0 ? -e : 0, len = TILE - (e < 0 ? -e : e);
+            #pragma unroll
+            for (int l = 0; l < NL; ++l) prev[l] = dS[l * LS + j0 * DSTR + i0];
+            for (int k = 0; k < len; ++k)
+                jstep<NL>(dS, wP, vS, vokS, (j0 + k + 1) * DSTR + i0 + k + 1, (j0 + k) * CSTR + i0 + k, prev, ch);
+            #pragma unroll
+            for (int l = 0; l < NL; ++l) prev[l] = dS[l * LS + (j0 + len + 1) * DSTR + i0 + len + 1];
+            for (int k = len - 1; k >= 0; --k)
+                jstep<NL>(dS, wP, vS, vokS, (j0 + k + 1) * DSTR + i0 + k + 1, (j0 + k) * CSTR + i0 + k, prev, ch);
+        }
+    } else if (warp < 6) {      // anti-diagonals i + j = s: (-,+) with j rising, then (+,-) with i rising
+        const int s = (warp - 4) * 32 + lane;
+        if (s <= 2 * TILE - 2) {
+            const uint32_t* wP = wS + S.plane_d * S.nl * WLS;
+            const int lo = s > TILE - 1 ? s - (TILE - 1) : 0;
+            const int len = TILE - (s > TILE - 1 ? s - (TILE - 1) : (TILE - 1) - s);
+            #pragma unroll
+            for (int l = 0; l < NL; ++l) prev[l] = dS[l * LS + lo * DSTR + (s - lo + 2)];
+            for (int k = 0; k < len; ++k) {
+                const int j = lo + k, i = s - j;
+                jstep<NL>(dS, wP, vS, vokS, (j + 1) * DSTR + i + 1, j * CSTR + i, prev, ch);
+            }
+            #pragma unroll
+            for (int l = 0; l < NL; ++l) prev[l] = dS[l * LS + (s - lo + 2) * DSTR + lo];
+            for (int k = 0; k < len; ++k) {
+                const int i = lo + k, j = s - i;
+                jstep<NL>(dS, wP, vS, vokS, (j + 1) * DSTR + i + 1, j * CSTR + i, prev, ch);
+            }
+        }
+    }
+    return ch;
+}
+
+template <int NL>
+__device__ int relax_joint(const SDev& S, uint32_t* dS, const uint32_t* wS, const uint32_t* vS, const uint32_t* vokS,
+                           VisitShared& sh, bool& requeue) {
+    for (int it = 0;; ++it) {
+        const int ch = joint_pass<NL>(S, dS, wS, vS, vokS);
+        const int any = __syncthreads_or(ch);
+        if (!any) return it + 1;
+        if (threadIdx.x == 0) sh.any = 1;
+        if (it + 1 >= MAX_IT) { requeue = true; return it + 1; }
+    }
+}
+
+// ---- per-layer scans with weights computed per move (mode 0: any factors, 64-bit distances) ----
+
+template <typename DT>
+__device__ int relax_general(const SDev& S, DT* dS, const float* cS, const DT* vS, const uint32_t* vokS,
+                             VisitShared& sh, bool& requeue) {
+    const int tid = threadIdx.x, nl = S.nl;
+    for (int it = 0;; ++it) {
+        int ch = 0;
+        for (int line = tid; line < nl * TILE; line += NT) {      // rows: +x, -x
+            const int l = line >> 5, r = line & 31;
+            DT* row = dS + l * LS + (r + 1) * DSTR;
+            const float* crow = cS + l * WLS + r * CSTR;
+            DT prev = row[0];
+            for (int k = 0; k < TILE; ++k) {
+                const DT v = row[k + 1], n = dmin(v, prev + qweight<DT>(crow[k], S.fac[l][0]));
+                if (n < v) { row[k + 1] = n; ch = 1; }
+                prev = n;
+            }
+            prev = row[TILE + 1];
+            for (int k = TILE - 1; k >= 0; --k) {
+                const DT v = row[k + 1], n = dmin(v, prev + qweight<DT>(crow[k], S.fac[l][1]));
+                if (n < v) { row[k + 1] = n; ch = 1; }
+                prev = n;
+            }
+        }
+        __syncthreads();
+        for (int line = tid; line < nl * TILE; line += NT) {      // columns: +y, -y
+            const int l = line >> 5, c = line & 31;
+            DT* col = dS + l * LS + c + 1;
+            const float* ccol = cS + l * WLS + c;
+            DT prev = col[0];
+            for (int k = 0; k < TILE; ++k) {
+                const DT v = col[(k + 1) * DSTR], n = dmin(v, prev + qweight<DT>(ccol[k * CSTR], S.fac[l][2]));
+                if (n < v) { col[(k + 1) * DSTR] = n; ch = 1; }
+                prev = n;
+            }
+            prev = col[(TILE + 1) * DSTR];
+            for (int k = TILE - 1; k >= 0; --k) {
+                const DT v = col[(k + 1) * DSTR], n = dmin(v, prev + qweight<DT>(ccol[k * CSTR], S.fac[l][3]));
+                if (n < v) { col[(k + 1) * DSTR] = n; ch = 1; }
+                prev = n;
+            }
+        }
+        __syncthreads();
+        for (int line = tid; line < nl * (2 * TILE - 1); line += NT) {   // i - j = e: (+,+), (-,-)
+            const int l = line / (2 * TILE - 1), e = line % (2 * TILE - 1) - (TILE - 1);
+            const int i0 = e > 0 ? e : 0, j0 = e < 0 ? -e : 0, len = TILE - (e < 0 ? -e : e);
+            DT* base = dS + l * LS;
+            const float* cb = cS + l * WLS;
+            DT prev = base[j0 * DSTR + i0];
+            for (int k = 0; k < len; ++k) {
+                DT* p = base + (j0 + k + 1) * DSTR + i0 + k + 1;
+                const DT v = *p, n = dmin(v, prev + qweight<DT>(cb[(j0 + k) * CSTR + i0 + k], S.fac[l][4]));
+                if (n < v) { *p = n; ch = 1; }
+                prev = n;
+            }
+            prev = base[(j0 + len + 1) * DSTR + i0 + len + 1];
+            for (int k = len - 1; k >= 0; --k) {
+                DT* p = base + (j0 + k + 1) * DSTR + i0 + k + 1;
+                const DT v = *p, n = dmin(v, prev + qweight<DT>(cb[(j0 + k) * CSTR + i0 + k], S.fac[l][7]));
+                if (n < v) { *p = n; ch = 1; }
+                prev = n;
+            }
+        }
+        __syncthreads();
+        for (int line = tid; line < nl * (2 * TILE - 1); line += NT) {   // i + j = s: (-,+), (+,-)
+            const int l = line / (2 * TILE - 1), s = line % (2 * TILE - 1);
+            const int lo = s > TILE - 1 ? s - (TILE - 1) : 0;
+            const int len = TILE - (s > TILE - 1 ? s - (TILE - 1) : (TILE - 1) - s);
+            DT* base = dS + l * LS;
+            const float* cb = cS + l * WLS;
+            DT prev = base[lo * DSTR + (s - lo + 2)];
+            for (int k = 0; k < len; ++k) {
+                const int j = lo + k, i = s - j;
+                DT* p = base + (j + 1) * DSTR + i + 1;
+                const DT v = *p, n = dmin(v, prev + qweight<DT>(cb[j * CSTR + i], S.fac[l][6]));
+                if (n < v) { *p = n; ch = 1; }
+                prev = n;
+            }
+            prev = base[(s - lo + 2) * DSTR + lo];
+            for (int k = 0; k < len; ++k) {
+                const int i = lo + k, j = s - i;
+                DT* p = base + (j + 1) * DSTR + i + 1;
+                const DT v = *p, n = dmin(v, prev + qweight<DT>(cb[j * CSTR + i], S.fac[l][5]));
+                if (n < v) { *p = n; ch = 1; }
+                prev = n;
+            }
+        }
+        __syncthreads();
+        for (int cell = tid; cell < TILE * TILE; cell += NT) {           // vias
+            const int r = cell >> 5, c = cell & 31;
+            const DT wv = vS[r * CSTR + c];
+            const uint32_t vm = vokS[r * CSTR + c];
+            if (wv >= Lim<DT>::INF || !vm) continue;
+            DT best = Lim<DT>::INF;
+            for (int l = 0; l < nl; ++l) best = dmin(best, dS[l * LS + (r + 1) * DSTR + c + 1]);
+            if (best >= Lim<DT>::INF) continue;
+            const DT n = best + wv;
+            for (int l = 0; l < nl; ++l) {
+                if (!((vm >> l) & 1)) continue;
+                DT* p = dS + l * LS + (r + 1) * DSTR + c + 1;
+                if (n < *p) { *p = n; ch = 1; }
+            }
+        }
+        const int any = __syncthreads_or(ch);
+        if (!any) return it + 1;
+        if (tid == 0) sh.any = 1;
+        if (it + 1 >= MAX_IT) { requeue = true; return it + 1; }
+    }
+}
+
+// ---- one tile visit ----
+
 template <typename DT>
 __device__ void visit_tile(const SolveArgs& a, int s, int tile, int round, unsigned char* smem) {
     const SDev& S = a.S[s];
@@ -135,256 +420,138 @@ __device__ void visit_tile(const SolveArgs& a, int s, int tile, int round, unsig
     const int nl = S.nl, pitch = S.pitch, hpad = S.hpad;
     const int tx = tile % S.ntx, ty = tile / S.ntx;
     const int x0 = tx * TILE, y0 = ty * TILE;
-    const SmemLayout L = smem_layout(a.nlmax, sizeof(DT));
+    const bool joint = sizeof(DT) == 4 && S.mode == 1;
+    const Lay L = layout_for(a.nlmax, a.kmax, sizeof(DT), joint ? 1 : 0);
     DT* dS = reinterpret_cast<DT*>(smem + L.d);
-    float* cS = reinterpret_cast<float*>(smem + L.c);
-    DT* wS = reinterpret_cast<DT*>(smem + L.w);
+    DT* vS = reinterpret_cast<DT*>(smem + L.v);
     DT* eS = reinterpret_cast<DT*>(smem + L.e);
-    uint8_t* vokS = smem + L.m;
-    uint8_t* tgS = vokS + TILE * CSTR;
-    __shared__ unsigned int sh_marks, sh_any;
-    __shared__ unsigned long long sh_tmin, sh_wmax;
-    __shared__ unsigned int sh_wide;
+    uint32_t* vokS = reinterpret_cast<uint32_t*>(smem + L.m);
+    uint32_t* tgS = vokS + WLS;
+    __shared__ VisitShared sh;
     const DT INF = Lim<DT>::INF;
-    const DT* dist = reinterpret_cast<const DT*>(S.dist);
-    DT* distw = reinterpret_cast<DT*>(S.dist);
-    if (tid == 0) { sh_marks = 0; sh_any = 0; sh_tmin = ~0ull; sh_wmax = 0; sh_wide = 0; }
+    if (tid == 0) { sh.marks = 0; sh.any = 0; sh.wide = 0; sh.iters = 0; sh.tmin = ~0ull; sh.wmax = 0; }
 
-    // ---- stage: distances with halo
-    for (int idx = tid; idx < nl * HS * HS; idx += NT) {
-        const int l = idx / (HS * HS), rem = idx % (HS * HS), r = rem / HS, c = rem % HS;
-        const int gy = y0 + r - 1, gx = x0 + c - 1;
-        DT v = INF;
-        if (gy >= 0 && gy < hpad && gx >= 0 && gx < pitch) v = dist[(size_t(l) * hpad + gy) * pitch + gx];
-        dS[(l * HS + r) * DSTR + c] = v;
-    }
-    // cost factors; the largest weight any move into a staged state can take decides whether 32-bit
-    // arithmetic is exact for this search
+    // ---- stage
+    stage_dist<DT>(S, dS, x0, y0);
     unsigned long long wmax = 0;
     bool wide = false;
-    for (int idx = tid; idx < nl * TILE * TILE; idx += NT) {
-        const int l = idx >> 10, r = (idx >> 5) & 31, c = idx & 31;
-        const float cf = S.cf[(size_t(l) * hpad + y0 + r) * pitch + x0 + c];
-        cS[(l * TILE + r) * CSTR + c] = cf;
-        if (cf < 1e30f) {
-            const float y = __fmul_rn(__fmul_rn(cf, S.maxfac[l]), 16.0f);
-            if (!(y < Lim<DT>::wlim())) wide = true;
-            else wmax = max(wmax, static_cast<unsigned long long>(qweight<DT>(cf, S.maxfac[l])));
-        }
-    }
-    // per cell: via weight and the via-landing / target masks over the layers
-    for (int cell = tid; cell < TILE * TILE; cell += NT) {
-        const int r = cell >> 5, c = cell & 31;
-        DT wv = INF;
-        if (S.vcf) {
-            const float v = S.vcf[size_t(y0 + r) * pitch + x0 + c];
-            if (v < 1e30f) {
-                const float y = __fmul_rn(v, 16.0f);
-                if (!(y < Lim<DT>::wlim())) wide = true;
-                else { wv = qweight<DT>(v, 1.0f); wmax = max(wmax, static_cast<unsigned long long>(wv)); }
+    if (joint) {
+        // integer weights of the x, y and diagonal move classes of every state
+        uint32_t* wS = reinterpret_cast<uint32_t*>(smem + L.w);
+        for (int idx = tid; idx < nl * TILE * TILE; idx += NT) {
+            const int l = idx >> 10, r = (idx >> 5) & 31, c = idx & 31;
+            const float cf = S.cf[(size_t(l) * hpad + y0 + r) * pitch + x0 + c];
+            if (cf < 1e30f && !(__fmul_rn(__fmul_rn(cf, S.maxfac[l]), 16.0f) < WLIM32)) wide = true;
+            const uint32_t wx = qweight<uint32_t>(cf, S.fac[l][0]), wy = qweight<uint32_t>(cf, S.fac[l][2]);
+            const uint32_t wd = qweight<uint32_t>(cf, S.fac[l][4]);
+            const int o = l * WLS + r * CSTR + c;
+            wS[o] = wx;
+            if (S.K == 3) wS[nl * WLS + o] = wy;
+            wS[(S.K - 1) * nl * WLS + o] = wd;
+            if (cf < 1e30f) {
+                const uint32_t mw = max(max(wx < INF32 ? wx : 0u, wy < INF32 ? wy : 0u), wd < INF32 ? wd : 0u);
+                wmax = max(wmax, static_cast<unsigned long long>(mw));
             }
         }
-        wS[r * CSTR + c] = wv;
-        unsigned int vm = 0, tm = 0;
-        for (int l = 0; l < nl; ++l) {
-            const uint8_t f = S.fl[(size_t(l) * hpad + y0 + r) * pitch + x0 + c];
-            vm |= unsigned(f & 1) << l;
-            tm |= unsigned((f >> 1) & 1) << l;
+    } else {
+        float* cS = reinterpret_cast<float*>(smem + L.w);
+        for (int idx = tid; idx < nl * TILE * TILE; idx += NT) {
+            const int l = idx >> 10, r = (idx >> 5) & 31, c = idx & 31;
+            const float cf = S.cf[(size_t(l) * hpad + y0 + r) * pitch + x0 + c];
+            cS[l * WLS + r * CSTR + c] = cf;
+            if (cf < 1e30f) {
+                const float y = __fmul_rn(__fmul_rn(cf, S.maxfac[l]), 16.0f);
+                if (!(y < Lim<DT>::wlim())) wide = true;
+                else wmax = max(wmax, static_cast<unsigned long long>(qweight<DT>(cf, S.maxfac[l])));
+            }
         }
-        vokS[r * CSTR + c] = uint8_t(vm);
-        tgS[r * CSTR + c] = uint8_t(tm);
     }
+    stage_cells<DT>(S, vS, vokS, tgS, x0, y0, wide, wmax);
     __syncthreads();
-    // original edge values (to tell which neighbours must look again)
-    for (int idx = tid; idx < nl * 4 * TILE; idx += NT) {
-        const int l = idx / (4 * TILE), side = (idx / TILE) & 3, k = idx % TILE;
-        const int r = side == 0 ? k : side == 1 ? k : side == 2 ? 0 : TILE - 1;
-        const int c = side == 0 ? 0 : side == 1 ? TILE - 1 : k;
-        eS[idx] = dS[(l * HS + r + 1) * DSTR + c + 1];
-    }
-    if (wide) atomicOr(&sh_wide, 1u);
-    if (wmax) atomicMax(&sh_wmax, wmax);
+    save_edges<DT>(S, dS, eS);
+    if (wide) atomicOr(&sh.wide, 1u);
+    if (wmax) atomicMax(&sh.wmax, wmax);
     __syncthreads();
 
     // ---- relax to a local fixed point
     bool requeue = false;
-    for (int it = 0;; ++it) {
-        int ch = 0;
-        // +x then -x along rows: one thread per (layer, row)
-        {
-            const int l = tid >> 5, r = tid & 31;
-            if (l < nl) {
-                DT* row = dS + (l * HS + r + 1) * DSTR;
-                const float* crow = cS + (l * TILE + r) * CSTR;
-                const float f0 = S.fac[l][0], f1 = S.fac[l][1];
-                DT prev = row[0];
-                #pragma unroll 8
-                for (int k = 0; k < TILE; ++k) {
-                    const DT v = row[k + 1], n = dmin(v, prev + qweight<DT>(crow[k], f0));
-                    if (n < v) { row[k + 1] = n; ch = 1; }
-                    prev = n;
-                }
-                prev = row[TILE + 1];
-                #pragma unroll 8
-                for (int k = TILE - 1; k >= 0; --k) {
-                    const DT v = row[k + 1], n = dmin(v, prev + qweight<DT>(crow[k], f1));
-                    if (n < v) { row[k + 1] = n; ch = 1; }
-                    prev = n;
-                }
-            }
+    int iters;
+    if (joint) {
+        const uint32_t* wS = reinterpret_cast<const uint32_t*>(smem + L.w);
+        uint32_t* d32 = reinterpret_cast<uint32_t*>(dS);
+        const uint32_t* v32 = reinterpret_cast<const uint32_t*>(vS);
+        switch (nl) {
+            case 1: iters = relax_joint<1>(S, d32, wS, v32, vokS, sh, requeue); break;
+            case 2: iters = relax_joint<2>(S, d32, wS, v32, vokS, sh, requeue); break;
+            case 3: iters = relax_joint<3>(S, d32, wS, v32, vokS, sh, requeue); break;
+            case 4: iters = relax_joint<4>(S, d32, wS, v32, vokS, sh, requeue); break;
+            case 5: iters = relax_joint<5>(S, d32, wS, v32, vokS, sh, requeue); break;
+            case 6: iters = relax_joint<6>(S, d32, wS, v32, vokS, sh, requeue); break;
+            case 7: iters = relax_joint<7>(S, d32, wS, v32, vokS, sh, requeue); break;
+            default: iters = relax_joint<8>(S, d32, wS, v32, vokS, sh, requeue); break;
         }
-        __syncthreads();
-        // +y then -y along columns: one thread per (layer, column)
-        {
-            const int l = tid >> 5, c = tid & 31;
-            if (l < nl) {
-                DT* col = dS + l * HS * DSTR + c + 1;
-                const float* ccol = cS + l * TILE * CSTR + c;
-                const float f2 = S.fac[l][2], f3 = S.fac[l][3];
-                DT prev = col[0];
-                #pragma unroll 8
-                for (int k = 0; k < TILE; ++k) {
-                    const DT v = col[(k + 1) * DSTR], n = dmin(v, prev + qweight<DT>(ccol[k * CSTR], f2));
-                    if (n < v) { col[(k + 1) * DSTR] = n; ch = 1; }
-                    prev = n;
-                }
-                prev = col[(TILE + 1) * DSTR];
-                #pragma unroll 8
-                for (int k = TILE - 1; k >= 0; --k) {
-                    const DT v = col[(k + 1) * DSTR], n = dmin(v, prev + qweight<DT>(ccol[k * CSTR], f3));
-                    if (n < v) { col[(k + 1) * DSTR] = n; ch = 1; }
-                    prev = n;
-                }
-            }
-        }
-        __syncthreads();
-        // main diagonals i - j = e: (+,+) forward, (-,-) backward
-        for (int line = tid; line < nl * (2 * TILE - 1); line += NT) {
-            const int l = line / (2 * TILE - 1), e = line % (2 * TILE - 1) - (TILE - 1);
-            const int i0 = e > 0 ? e : 0, j0 = e < 0 ? -e : 0, len = TILE - (e < 0 ? -e : e);
-            DT* base = dS + l * HS * DSTR;
-            const float* cb = cS + l * TILE * CSTR;
-            const float f4 = S.fac[l][4], f7 = S.fac[l][7];
-            DT prev = base[j0 * DSTR + i0];  // (i0 - 1, j0 - 1) in halo coordinates
-            for (int k = 0; k < len; ++k) {
-                const int i = i0 + k, j = j0 + k;
-                DT* p = base + (j + 1) * DSTR + i + 1;
-                const DT v = *p, n = dmin(v, prev + qweight<DT>(cb[j * CSTR + i], f4));
-                if (n < v) { *p = n; ch = 1; }
-                prev = n;
-            }
-            prev = base[(j0 + len + 1) * DSTR + i0 + len + 1];
-            for (int k = len - 1; k >= 0; --k) {
-                const int i = i0 + k, j = j0 + k;
-                DT* p = base + (j + 1) * DSTR + i + 1;
-                const DT v = *p, n = dmin(v, prev + qweight<DT>(cb[j * CSTR + i], f7));
-                if (n < v) { *p = n; ch = 1; }
-                prev = n;
-            }
-        }
-        __syncthreads();
-        // anti-diagonals i + j = s: (-,+) with j increasing, (+,-) with i increasing
-        for (int line = tid; line < nl * (2 * TILE - 1); line += NT) {
-            const int l = line / (2 * TILE - 1), sdx = line % (2 * TILE - 1);
-            const int lo = sdx > TILE - 1 ? sdx - (TILE - 1) : 0, len = TILE - (sdx > TILE - 1 ? sdx - (TILE - 1) : (TILE - 1) - sdx);
-            DT* base = dS + l * HS * DSTR;
-            const float* cb = cS + l * TILE * CSTR;
-            const float f5 = S.fac[l][5], f6 = S.fac[l][6];
-            // (-,+): q = (i, j) from p = (i + 1, j - 1); cells j = lo .. lo + len - 1, i = sdx - j
-            {
-                DT prev = base[lo * DSTR + (sdx - lo + 1) + 1];
-                for (int k = 0; k < len; ++k) {
-                    const int j = lo + k, i = sdx - j;
-                    DT* p = base + (j + 1) * DSTR + i + 1;
-                    const DT v = *p, n = dmin(v, prev + qweight<DT>(cb[j * CSTR + i], f6));
-                    if (n < v) { *p = n; ch = 1; }
-                    prev = n;
-                }
-            }
-            // (+,-): q = (i, j) from p = (i - 1, j + 1); cells i = lo .. lo + len - 1, j = sdx - i
-            {
-                DT prev = base[(sdx - lo + 1 + 1) * DSTR + lo];
-                for (int k = 0; k < len; ++k) {
-                    const int i = lo + k, j = sdx - i;
-                    DT* p = base + (j + 1) * DSTR + i + 1;
-                    const DT v = *p, n = dmin(v, prev + qweight<DT>(cb[j * CSTR + i], f5));
-                    if (n < v) { *p = n; ch = 1; }
-                    prev = n;
-                }
-            }
-        }
-        __syncthreads();
-        // vias: from the cheapest layer of a cell to every layer a via may land on
-        for (int cell = tid; cell < TILE * TILE; cell += NT) {
-            const int r = cell >> 5, c = cell & 31;
-            const DT wv = wS[r * CSTR + c];
-            if (wv >= INF) continue;
-            const unsigned int vm = vokS[r * CSTR + c];
-            if (!vm) continue;
-            DT best = INF;
-            for (int l = 0; l < nl; ++l) best = dmin(best, dS[(l * HS + r + 1) * DSTR + c + 1]);
-            if (best >= INF) continue;
-            const DT n = best + wv;
-            for (int l = 0; l < nl; ++l) {
-                if (!((vm >> l) & 1)) continue;
-                DT* p = dS + (l * HS + r + 1) * DSTR + c + 1;
-                if (n < *p) { *p = n; ch = 1; }
-            }
-        }
-        const int any = __syncthreads_or(ch);
-        if (!any) break;
-        if (tid == 0) sh_any = 1;
-        if (it + 1 >= MAX_IT) { requeue = true; break; }
+    } else {
+        iters = relax_general<DT>(S, dS, reinterpret_cast<const float*>(smem + L.w), vS, vokS, sh, requeue);
     }
     __syncthreads();
 
-    // ---- targets of the tile: least (distance) into the search's bound
+    // ---- targets of the tile: least distance into the search's bound
     const unsigned long long ub_now = *reinterpret_cast<volatile unsigned long long*>(&a.st[s].ub);
     {
         unsigned long long tmin = ~0ull;
         for (int cell = tid; cell < TILE * TILE; cell += NT) {
             const int r = cell >> 5, c = cell & 31;
-            const unsigned int tm = tgS[r * CSTR + c];
+            const uint32_t tm = tgS[r * CSTR + c];
             if (!tm) continue;
             for (int l = 0; l < nl; ++l)
                 if ((tm >> l) & 1) {
-                    const DT v = dS[(l * HS + r + 1) * DSTR + c + 1];
+                    const DT v = dS[l * LS + (r + 1) * DSTR + c + 1];
                     if (v < INF) tmin = min(tmin, static_cast<unsigned long long>(v));
                 }
         }
-        if (tmin != ~0ull) atomicMin(&sh_tmin, tmin);
+        if (tmin != ~0ull) atomicMin(&sh.tmin, tmin);
     }
     __syncthreads();
-    const unsigned long long ub = min(ub_now, sh_tmin);
-    if (sh_any) {
-        // write back the interior
+    const unsigned long long ub = min(ub_now, sh.tmin);
+    if (sh.any) {
+        DT* distw = reinterpret_cast<DT*>(S.dist);
         for (int idx = tid; idx < nl * TILE * TILE; idx += NT) {
             const int l = idx >> 10, r = (idx >> 5) & 31, c = idx & 31;
-            distw[(size_t(l) * hpad + y0 + r) * pitch + x0 + c] = dS[(l * HS + r + 1) * DSTR + c + 1];
+            distw[(size_t(l) * hpad + y0 + r) * pitch + x0 + c] = dS[l * LS + (r + 1) * DSTR + c + 1];
         }
-        // edges that improved to at most the bound: the neighbours reading them look again
+        // an edge cell that improved (to at most the bound) below an adjacent neighbour cell's staged value:
+        // that neighbour looks again. bits: 0 L, 1 R, 2 T, 3 B, 4 TL, 5 TR, 6 BL, 7 BR
         unsigned int marks = 0;
         for (int idx = tid; idx < nl * 4 * TILE; idx += NT) {
             const int l = idx / (4 * TILE), side = (idx / TILE) & 3, k = idx % TILE;
-            const int r = side == 0 ? k : side == 1 ? k : side == 2 ? 0 : TILE - 1;
-            const int c = side == 0 ? 0 : side == 1 ? TILE - 1 : k;
-            const DT v = dS[(l * HS + r + 1) * DSTR + c + 1];
+            int r, c;
+            edge_rc(side, k, r, c);
+            const DT v = dS[l * LS + (r + 1) * DSTR + c + 1];
             if (!(v < eS[idx]) || static_cast<unsigned long long>(v) > ub) continue;
-            // bits: 0 L, 1 R, 2 T, 3 B, 4 TL, 5 TR, 6 BL, 7 BR
-            if (side == 0) { marks |= 1u; if (k == 0) marks |= 16u; if (k == TILE - 1) marks |= 64u; }
-            else if (side == 1) { marks |= 2u; if (k == 0) marks |= 32u; if (k == TILE - 1) marks |= 128u; }
-            else if (side == 2) marks |= 4u;
-            else marks |= 8u;
+            const DT* hb = dS + l * LS;
+            // the three halo cells across this side, and the neighbour tile each belongs to
+            for (int t = -1; t <= 1; ++t) {
+                int hr, hc, bit;
+                if (side == 0 || side == 1) {
+                    hr = r + t; hc = side == 0 ? -1 : TILE;
+                    bit = hr < 0 ? (side == 0 ? 4 : 5) : hr >= TILE ? (side == 0 ? 6 : 7) : side;
+                } else {
+                    hc = c + t; hr = side == 2 ? -1 : TILE;
+                    bit = hc < 0 ? (side == 2 ? 4 : 6) : hc >= TILE ? (side == 2 ? 5 : 7) : side;
+                }
+                if (v < hb[(hr + 1) * DSTR + hc + 1]) marks |= 1u << bit;
+            }
         }
-        if (marks) atomicOr(&sh_marks, marks);
+        if (marks) atomicOr(&sh.marks, marks);
     }
+    if (tid == 0) sh.iters = unsigned(iters);
     __syncthreads();
     if (tid == 0) {
         SStat& st = a.st[s];
-        if (sh_tmin != ~0ull && sh_tmin < ub_now) atomicMin(&st.ub, sh_tmin);
-        if (sh_wmax) atomicMax(&st.maxw, sh_wmax);
-        if (sh_wide) atomicOr(&st.need_wide, 1u);
-        const unsigned int m = sh_marks;
+        if (sh.tmin != ~0ull && sh.tmin < ub_now) atomicMin(&st.ub, sh.tmin);
+        if (sh.wmax) atomicMax(&st.maxw, sh.wmax);
+        if (sh.wide) atomicOr(&st.need_wide, 1u);
+        const unsigned int m = sh.marks;
         const int DXs[8] = {-1, 1, 0, 0, -1, 1, -1, 1}, DYs[8] = {0, 0, -1, 1, -1, -1, 1, 1};
         for (int b = 0; b < 8; ++b) {
             if (!((m >> b) & 1)) continue;
@@ -394,6 +561,8 @@ __device__ void visit_tile(const SolveArgs& a, int s, int tile, int round, unsig
         }
         if (requeue) enqueue(a, S, s, tile, round + 1);
         atomicAdd(a.visits, 1ull);
+        atomicAdd(a.visits + 1, static_cast<unsigned long long>(nl));
+        atomicAdd(a.visits + 2, static_cast<unsigned long long>(sh.iters));
     }
     __syncthreads();
 }
@@ -447,7 +616,9 @@ __global__ void __launch_bounds__(NT) relax_kernel(SolveArgs a) {
     if (blockIdx.x == 0 && threadIdx.x == 0) a.ctl[C_ROUNDS] = unsigned(round);
 }
 
-// starts: distance init (least per state) and the first round's tiles
+// starts: distance init (least per state) and the first round's tiles. A start's value is written here, not by a
+// visit, so no visit sees it "improve": the tile holding it and all 8 neighbours (which read it through their
+// halo) are queued.
 template <typename DT>
 __global__ void seed_kernel(SolveArgs a, const uint32_t* const* sidx, const uint64_t* const* sd, const int* ns) {
     const int s = blockIdx.x;
@@ -461,7 +632,12 @@ __global__ void seed_kernel(SolveArgs a, const uint32_t* const* sidx, const uint
         uint64_t v = sd[s][k];
         if (v >= uint64_t(Lim<DT>::INF)) continue;
         atomic_min_d(dist + (size_t(l) * S.hpad + j) * S.pitch + i, DT(v));
-        enqueue(a, S, s, (j / TILE) * S.ntx + i / TILE, 1);
+        const int tx = i / TILE, ty = j / TILE;
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx) {
+                const int nx = tx + dx, ny = ty + dy;
+                if (nx >= 0 && ny >= 0 && nx < S.ntx && ny < S.nty) enqueue(a, S, s, ny * S.ntx + nx, 1);
+            }
     }
 }
 
@@ -518,15 +694,13 @@ struct DevBuf {
 
 struct Arena {
     DevBuf dist, stamp, wl, sdev, sstat, ctl, visits, sptr;
-    std::vector<unsigned char> hbuf;
 } g_arena;
 
 thread_local std::string t_err;
 thread_local BatchStats t_stats;
+cudaEvent_t g_ev0 = nullptr, g_ev1 = nullptr;
 
-template <typename DT> int occupancy_blocks(int nlmax, size_t* smem_out) {
-    const size_t smem = smem_layout(nlmax, sizeof(DT)).total;
-    *smem_out = smem;
+template <typename DT> int occupancy_blocks(size_t smem) {
     if (cudaFuncSetAttribute(relax_kernel<DT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess) return -1;
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, relax_kernel<DT>, NT, smem) != cudaSuccess) return -1;
@@ -536,14 +710,30 @@ template <typename DT> int occupancy_blocks(int nlmax, size_t* smem_out) {
     return per_sm * sms;
 }
 
-// Solve items[idx[0..m)] with DT distances. dist scratch per item at doff[k] (bytes).
+// joint mode needs one factor per move class on every layer (true of every query the router builds)
+void classify(SDev& S) {
+    bool ok = true, xy = true;
+    for (int l = 0; l < S.nl; ++l) {
+        const float* f = S.fac[l];
+        ok &= f[0] == f[1] && f[2] == f[3] && f[4] == f[5] && f[4] == f[6] && f[4] == f[7];
+        xy &= f[0] == f[2];
+    }
+    S.mode = ok ? 1 : 0;
+    S.K = xy ? 2 : 3;
+    S.plane_h = 0;
+    S.plane_v = xy ? 0 : 1;
+    S.plane_d = S.K - 1;
+}
+
+// Solve items[idx[0..m)] with DT distances.
 template <typename DT>
-int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream, int& rounds_out, long long& visits_out) {
+int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream, BatchStats& bs) {
     const int m = int(idx.size());
     std::vector<SDev> sd(m);
     std::vector<size_t> doff(m), toff(m);
     size_t dbytes = 0, tiles = 0;
-    int nlmax = 1;
+    int nlmax = 1, kmax = 0;
+    bool any_general = false;
     for (int k = 0; k < m; ++k) {
         const BatchItem& b = items[idx[k]];
         SDev& S = sd[k];
@@ -552,9 +742,13 @@ int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream
         S.ntx = b.pitch / TILE; S.nty = b.hpad / TILE;
         for (int l = 0; l < MAX_LAYERS; ++l) {
             float mf = 0.f;
-            for (int d = 0; d < 8; ++d) { S.fac[l][d] = b.fac[l][d]; mf = std::max(mf, b.fac[l][d]); }
+            for (int d = 0; d < 8; ++d) { S.fac[l][d] = b.fac[l][d]; if (l < b.nl) mf = std::max(mf, b.fac[l][d]); }
             S.maxfac[l] = mf;
         }
+        classify(S);
+        if (sizeof(DT) != 4) S.mode = 0;
+        if (S.mode) kmax = std::max(kmax, S.K);
+        else any_general = true;
         S.cf = b.cf; S.fl = b.fl; S.vcf = b.vcf; S.out = b.out;
         doff[k] = dbytes;
         dbytes += round_up(size_t(b.nl) * b.hpad * b.pitch * sizeof(DT), 256);
@@ -562,11 +756,14 @@ int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream
         tiles += size_t(S.ntx) * S.nty;
         nlmax = std::max(nlmax, b.nl);
     }
+    size_t smem = 0;
+    if (kmax) smem = std::max(smem, layout(nlmax, kmax, 4).total);
+    if (any_general) smem = std::max(smem, layout(nlmax, 1, sizeof(DT)).total);
     Arena& A = g_arena;
     const unsigned int cap = unsigned(std::max<size_t>(tiles, 1));
     if (!A.dist.need(dbytes) || !A.stamp.need(tiles * 4 + 4) || !A.wl.need(size_t(3) * cap * 8) ||
         !A.sdev.need(sizeof(SDev) * m) || !A.sstat.need(sizeof(SStat) * m) || !A.ctl.need(C_N * 4) ||
-        !A.visits.need(8) || !A.sptr.need(size_t(m) * (8 + 8 + 4) + 64)) {
+        !A.visits.need(24) || !A.sptr.need(size_t(m) * (8 + 8 + 4) + 64)) {
         t_err = "device allocation failed";
         return -1;
     }
@@ -574,7 +771,6 @@ int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream
         sd[k].dist = static_cast<unsigned char*>(A.dist.p) + doff[k];
         sd[k].stamp = static_cast<uint32_t*>(A.stamp.p) + toff[k];
     }
-    // host-side arrays for the start pointers
     std::vector<const uint32_t*> sip(m);
     std::vector<const uint64_t*> sdp(m);
     std::vector<int> nsv(m);
@@ -593,39 +789,49 @@ int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream
     cudaMemsetAsync(A.dist.p, 0x7F, dbytes, stream);
     cudaMemsetAsync(A.stamp.p, 0, tiles * 4 + 4, stream);
     cudaMemsetAsync(A.ctl.p, 0, C_N * 4, stream);
-    cudaMemsetAsync(A.visits.p, 0, 8, stream);
+    cudaMemsetAsync(A.visits.p, 0, 24, stream);
     SolveArgs a;
     a.S = static_cast<const SDev*>(A.sdev.p);
     a.st = static_cast<SStat*>(A.sstat.p);
     a.n = m;
     a.nlmax = nlmax;
+    a.kmax = kmax;
     a.wl = static_cast<unsigned long long*>(A.wl.p);
     a.cap = cap;
     a.ctl = static_cast<unsigned int*>(A.ctl.p);
     a.visits = static_cast<unsigned long long*>(A.visits.p);
     a.max_rounds = 1 << 20;
     seed_kernel<DT><<<m, 128, 0, stream>>>(a, d_sip, d_sdp, d_ns);
-    size_t smem = 0;
-    const int blocks = occupancy_blocks<DT>(nlmax, &smem);
+    const int blocks = occupancy_blocks<DT>(smem);
     if (blocks <= 0) { t_err = "relax kernel cannot be resident"; return -1; }
     void* args[] = {&a};
+    if (!g_ev0) { cudaEventCreate(&g_ev0); cudaEventCreate(&g_ev1); }
+    cudaEventRecord(g_ev0, stream);
     cudaError_t e = cudaLaunchCooperativeKernel(reinterpret_cast<void*>(relax_kernel<DT>), dim3(blocks), dim3(NT), args, smem, stream);
     if (e != cudaSuccess) { t_err = std::string("cooperative launch: ") + cudaGetErrorString(e); return -1; }
+    cudaEventRecord(g_ev1, stream);
     report_kernel<DT><<<dim3(32, m), 256, 0, stream>>>(a.S, a.st);
+    bs.launches += 3;
     std::vector<SStat> st(m);
     unsigned int ctl[C_N];
-    unsigned long long visits = 0;
+    unsigned long long visits[3] = {0, 0, 0};
     cudaMemcpyAsync(st.data(), A.sstat.p, sizeof(SStat) * m, cudaMemcpyDeviceToHost, stream);
     cudaMemcpyAsync(ctl, A.ctl.p, sizeof(ctl), cudaMemcpyDeviceToHost, stream);
-    cudaMemcpyAsync(&visits, A.visits.p, 8, cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(visits, A.visits.p, 24, cudaMemcpyDeviceToHost, stream);
     e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) { t_err = std::string("batch solve: ") + cudaGetErrorString(e); return -1; }
     if (ctl[C_ERR]) {
         t_err = "batch solve aborted (error bits " + std::to_string(ctl[C_ERR]) + ")";
         return -1;
     }
-    rounds_out = int(ctl[C_ROUNDS]);
-    visits_out = (long long)visits;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, g_ev0, g_ev1);
+    bs.kernel_ms += ms;
+    bs.rounds += int(ctl[C_ROUNDS]);
+    bs.tile_visits += (long long)visits[0];
+    bs.layer_visits += (long long)visits[1];
+    bs.local_iters += (long long)visits[2];
+    const int rounds_out = int(ctl[C_ROUNDS]);
     const unsigned long long INF = static_cast<unsigned long long>(Lim<DT>::INF);
     for (int k = 0; k < m; ++k) {
         BatchItem& b = items[idx[k]];
@@ -665,18 +871,12 @@ int solve_batch(BatchItem* items, int n, cudaStream_t stream) {
     }
     std::vector<int> all(n);
     for (int k = 0; k < n; ++k) all[k] = k;
-    int rounds = 0;
-    long long visits = 0;
-    if (run_batch<uint32_t>(items, all, stream, rounds, visits) != 0) return -1;
-    t_stats.rounds = rounds;
-    t_stats.tile_visits = visits;
+    if (run_batch<uint32_t>(items, all, stream, t_stats) != 0) return -1;
     std::vector<int> wide;
     for (int k = 0; k < n; ++k)
         if (items[k].status == 1) wide.push_back(k);
     if (!wide.empty()) {
-        if (run_batch<uint64_t>(items, wide, stream, rounds, visits) != 0) return -1;
-        t_stats.rounds += rounds;
-        t_stats.tile_visits += visits;
+        if (run_batch<uint64_t>(items, wide, stream, t_stats) != 0) return -1;
         for (int k : wide) items[k].status = 1;
     }
     return 0;
@@ -710,3 +910,7 @@ extern "C" int pcbg_solve_batch(pcbg_search* s, int32_t n, void* stream) {
 
 extern "C" int64_t pcbg_last_batch_tile_visits(void) { return pcbg::last_stats().tile_visits; }
 extern "C" int32_t pcbg_last_batch_rounds(void) { return pcbg::last_stats().rounds; }
+extern "C" int64_t pcbg_last_batch_layer_visits(void) { return pcbg::last_stats().layer_visits; }
+extern "C" float pcbg_last_batch_kernel_ms(void) { return pcbg::last_stats().kernel_ms; }
+extern "C" int32_t pcbg_last_batch_launches(void) { return pcbg::last_stats().launches; }
+extern "C" int64_t pcbg_last_batch_local_iters(void) { return pcbg::last_stats().local_iters; }

@@ -4,6 +4,8 @@
 // the same arrays bit for bit on the host.
 #include <algorithm>
 #include <cstdint>
+#include <thread>
+#include <vector>
 
 #include "pcbg_internal.h"
 
@@ -85,6 +87,45 @@ __global__ void pick_kernel(uint64_t seed, int rw, int rh, int nl, int pitch, in
 
 }  // namespace
 }  // namespace pcbg
+
+extern "C" int pcbg_synth_search_host(uint64_t seed, int32_t rw, int32_t rh, int32_t nl, float via, float* cf,
+                                      uint8_t* flags, float* vcf, int64_t* src_tgt, int32_t threads) {
+    using namespace pcbg;
+    if (nl < 1 || nl > MAX_LAYERS || rw < 1 || rh < 1) return PCBG_ERR_FAIL;
+    const size_t RN = size_t(rw) * rh;
+    auto rows = [&](int t, int nt) {
+        for (int row = t; row < rh * nl; row += nt) {
+            const int l = row / rh, j = row % rh;
+            for (int i = 0; i < rw; ++i) {
+                const size_t q = size_t(l) * RN + size_t(j) * rw + i;
+                const bool b = blocked(seed, l, i, j);
+                const uint64_t h = hash4(seed, 1, uint64_t(l), uint64_t(j) * rw + i);
+                cf[q] = b ? 1e30f : float(1 + int((h >> 32) % 16));
+                flags[q] = b ? 0 : 1;
+                if (l == 0 && vcf) vcf[size_t(j) * rw + i] = via;
+            }
+        }
+    };
+    const int nt = std::max(1, std::min(threads, rh * nl));
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; ++t) th.emplace_back(rows, t, nt);
+    rows(0, nt);
+    for (auto& x : th) x.join();
+    const uint64_t N = RN * nl;
+    int64_t src = -1, tgt = -1;
+    for (int k = 0; k < 64 && src < 0; ++k) {
+        const uint64_t c = hash4(seed, 4, uint64_t(k), 0) % N;
+        if (!blocked(seed, int(c / RN), int(c % rw), int((c % RN) / rw))) src = int64_t(c);
+    }
+    for (int k = 0; k < 64 && tgt < 0; ++k) {
+        const uint64_t c = hash4(seed, 5, uint64_t(k), 0) % N;
+        if (!blocked(seed, int(c / RN), int(c % rw), int((c % RN) / rw)) && int64_t(c) != src) tgt = int64_t(c);
+    }
+    if (tgt >= 0) flags[tgt] |= 2;
+    src_tgt[0] = src;
+    src_tgt[1] = tgt;
+    return 0;
+}
 
 extern "C" int pcbg_synth_search(uint64_t seed, int32_t rw, int32_t rh, int32_t nl, int32_t pitch, int32_t hpad, float via,
                                  float* cf, uint8_t* flags, float* vcf, int64_t* src_tgt, void* stream) {

@@ -132,7 +132,8 @@ def microbench_sizes(seed: int, n: int) -> list[tuple[int, int, int, float, int]
 
 def random_query(seed: int, nx: int = 96, ny: int = 80, nl: int = 3, *, window=None, prior: bool = False,
                  corridor: bool = False, vias: bool = True, n_starts: int = 3, n_targets: int = 4,
-                 own: bool = True, unusable_layer: bool = False, big_costs: bool = False) -> GpuQuery:
+                 own: bool = True, unusable_layer: bool = False, big_costs: bool = False,
+                 free_dirf: bool = False) -> GpuQuery:
     """A random search over a full grid of nx x ny x nl, as the router would hand it to gpu_solve."""
     rng = np.random.default_rng(seed)
     me = 7
@@ -172,6 +173,8 @@ def random_query(seed: int, nx: int = 96, ny: int = 80, nl: int = 3, *, window=N
             dirf[l, :2] = 1.0 if pref == 1 else w
             dirf[l, 2:4] = w if pref == 1 else 1.0
             dirf[l, 4:] = wd
+    if free_dirf:  # a factor per move (no x / y / diagonal classes)
+        dirf[:nl] = (1.0 + rng.integers(0, 5, size=(nl, 8)) * 0.25).astype(np.float32)
     lay = np.zeros(8, np.uint8)
     lay[:nl] = 1
     if unusable_layer and nl > 1:

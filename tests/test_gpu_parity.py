@@ -150,6 +150,58 @@ def test_query_matches_oracle(gpu, seed, opts):
 
 
 @pytest.mark.parametrize("seed", range(4))
+def test_query_free_direction_factors(gpu, seed):
+    """A factor per move (no x / y / diagonal classes): the general per-layer relaxation."""
+    _cmp_query(synth.random_query(500 + seed, nx=110, ny=90, nl=2 + seed, free_dirf=True))
+
+
+@pytest.mark.parametrize("corner", [(31, 31), (32, 32), (31, 32), (0, 31), (63, 0), (32, 5), (5, 63)])
+def test_start_on_tile_edges(gpu, corner):
+    """Starts on tile edges and corners: the tiles around a start must all relax from it."""
+    i, j = corner
+    q = synth.random_query(600 + i + 7 * j, nx=100, ny=100, nl=2, window=(0, 0, 100, 100), n_starts=1, n_targets=2,
+                           own=False)
+    q.starts = [(j * q.ww + i, 0.0)]
+    _cmp_query(q)
+
+
+def test_batch_mixes_joint_and_general_searches(gpu):
+    """One persistent launch holding searches of both relaxation modes and different layer counts."""
+    torch = _torch()
+    lib = _lib.load()
+    searches = [make_device_search(4000 + k, 70 + 31 * k, 50 + 17 * k, 2 + k % 5, 9.0) for k in range(6)]
+    arr = (_lib.Search * len(searches))()
+    keep, facs = [], []
+    rng = np.random.default_rng(3)
+    for k, s in enumerate(searches):
+        a = arr[k]
+        a.rw, a.rh, a.nl, a.pitch, a.hpad = s["rw"], s["rh"], s["nl"], s["pitch"], s["hpad"]
+        fac = synth.microbench_factors(s["nl"])
+        if k % 2:  # per-move factors: general mode
+            fac = (fac * (1.0 + rng.integers(0, 4, size=(8, 8)) * 0.25)).astype(np.float32)
+        facs.append(fac)
+        for l in range(8):
+            for m in range(8):
+                a.fac[l][m] = float(fac[l, m])
+        a.cf, a.flags, a.vcf = s["cf"].data_ptr(), s["fl"].data_ptr(), s["vcf"].data_ptr()
+        si = s["st"][:1].to(torch.int32)
+        sd = torch.zeros(1, dtype=torch.int64, device="cuda")
+        out = torch.empty(s["nl"] * s["rh"] * s["rw"], dtype=torch.float32, device="cuda")
+        keep += [si, sd, out]
+        s["out"] = out
+        a.start_idx, a.start_d, a.n_starts, a.out = si.data_ptr(), sd.data_ptr(), 1, out.data_ptr()
+    assert lib.pcbg_solve_batch(arr, len(arr), None) == 0, _lib.last_error()
+    torch.cuda.synchronize()
+    for k, s in enumerate(searches):
+        cf, fl, vcf, src, tgt = synth.search_arrays(s["seed"], s["rw"], s["rh"], s["nl"], s["via"])
+        dist, best, bd = oracle.dijkstra(facs[k], cf, fl, vcf, np.array([src], np.uint32), np.zeros(1, np.uint64))
+        field = oracle.report(dist, best, bd)
+        assert arr[k].best == best
+        got = s["out"].cpu().numpy().reshape(s["nl"], s["rh"], s["rw"])
+        assert np.array_equal(got.view(np.uint32), field.view(np.uint32)), k
+
+
+@pytest.mark.parametrize("seed", range(4))
 def test_query_rectangle_growth(gpu, seed):
     """Windows much larger than the start/target box: the solved rectangle grows by 80 x 3^k cells."""
     rng = np.random.default_rng(seed)
