@@ -122,6 +122,29 @@ typedef struct pcbg_search {
  * the results are in the structs. */
 int pcbg_solve_batch(pcbg_search* s, int32_t n, void* stream);
 
+/* Largest search (padded states, nl * hpad * pitch) pcbg_solve_noalloc accepts. */
+#define PCBG_NOALLOC_MAX_STATES 2097152
+
+/* Solve one resolved device search without allocating any memory. No counterpart in the reference.
+ *
+ * Some callers cannot call cudaMalloc / cudaFree:
+ *   - a host process whose device memory is owned by another allocator, for example a framework's caching pool or
+ *     a fixed per-process budget, so that any memory outside it is refused;
+ *   - a host thread that must not stall its peers: cudaFree waits for all work on the device, so the batch path's
+ *     growing arena can pause every other router thread's searches at an unpredictable moment.
+ * This entry point takes the same pcbg_search as pcbg_solve_batch: inputs, starts and the optional output field
+ * are still the caller's. All scratch (distances, tile stamps and worklists, descriptors) lives in one static
+ * device array, sized for PCBG_NOALLOC_MAX_STATES padded states. That is about 16.1 MiB, and every GPU that
+ * loads the library holds it until the process exits. Larger searches return PCBG_ERR_FAIL with the reason in
+ * pcbg_last_error(). The call itself makes no cudaMalloc, cudaFree or allocating library call.
+ *
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress). Make that first call
+ * before any stream capture. Every call shares the one array and clears what it needs at the start. Calls
+ * whose GPU work overlaps would race on the array, so this function serialises calls within the process and
+ * returns only when its work on `stream` is done. Returns 0 (results in *s, as pcbg_solve_batch) or
+ * PCBG_ERR_FAIL. */
+int pcbg_solve_noalloc(pcbg_search* s, void* stream);
+
 /* Counters of the last batch solved on this thread (for throughput and roofline accounting): tile visits, the sum
  * over visits of the search's layer count (each layer of a visit stages 32 x 32 states), relaxation rounds, the
  * device time of the relaxation launches in ms (CUDA events on the launch stream), and kernels launched. */

@@ -15,7 +15,7 @@ LIB_PATH = _build.LIB
 # the symbols include/pcbg.h declares (C linkage) and include/gpu.h declares (C++ linkage, mangled)
 PCBG_SYMBOLS = [
     "pcbg_available", "pcbg_configure", "pcbg_solve", "pcbg_host_acquire", "pcbg_host_release", "pcbg_last_error",
-    "pcbg_solve_batch", "pcbg_last_batch_tile_visits", "pcbg_last_batch_layer_visits", "pcbg_last_batch_rounds",
+    "pcbg_solve_batch", "pcbg_solve_noalloc", "pcbg_last_batch_tile_visits", "pcbg_last_batch_layer_visits", "pcbg_last_batch_rounds",
     "pcbg_last_batch_kernel_ms", "pcbg_last_batch_launches", "pcbg_last_batch_local_iters", "pcbg_synth_search", "pcbg_synth_search_host",
 ]
 GPU_H_SYMBOLS = [
@@ -99,6 +99,8 @@ def load() -> C.CDLL:
     lib.pcbg_last_error.restype = C.c_char_p
     lib.pcbg_solve_batch.argtypes = [C.POINTER(Search), C.c_int32, C.c_void_p]
     lib.pcbg_solve_batch.restype = C.c_int
+    lib.pcbg_solve_noalloc.argtypes = [C.POINTER(Search), C.c_void_p]
+    lib.pcbg_solve_noalloc.restype = C.c_int
     lib.pcbg_last_batch_tile_visits.restype = C.c_int64
     lib.pcbg_last_batch_layer_visits.restype = C.c_int64
     lib.pcbg_last_batch_rounds.restype = C.c_int32

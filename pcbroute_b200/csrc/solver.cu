@@ -914,3 +914,150 @@ extern "C" int64_t pcbg_last_batch_layer_visits(void) { return pcbg::last_stats(
 extern "C" float pcbg_last_batch_kernel_ms(void) { return pcbg::last_stats().kernel_ms; }
 extern "C" int32_t pcbg_last_batch_launches(void) { return pcbg::last_stats().launches; }
 extern "C" int64_t pcbg_last_batch_local_iters(void) { return pcbg::last_stats().local_iters; }
+
+// ---- pcbg_solve_noalloc: one search with all scratch in a static device array ----
+//
+// For callers that cannot allocate device memory. Everything the batch path takes from its grow-only arena
+// (distances, tile stamps, worklists, descriptors, control words) is carved here from one file-scope array of fixed
+// size instead, and the host side uses only stack storage.
+
+static __device__ __align__(256) unsigned char pcbg_noalloc_scratch[
+    PCBG_NOALLOC_MAX_STATES * 8 +                                          // distances, room for 64-bit
+    (PCBG_NOALLOC_MAX_STATES / (pcbg::TILE * pcbg::TILE)) * (4 + 3 * 8) +  // tile stamps, 3 worklists
+    4096];                                                                  // descriptors, control words
+
+namespace pcbg {
+namespace {
+
+constexpr size_t NA_TILES = PCBG_NOALLOC_MAX_STATES / (TILE * TILE);
+constexpr size_t NA_DIST = size_t(PCBG_NOALLOC_MAX_STATES) * 8;
+constexpr size_t NA_STAMP = NA_TILES * 4;
+constexpr size_t NA_WL = NA_TILES * 3 * 8;
+// offsets in the small area after the worklists
+constexpr size_t NA_SDEV = 0, NA_SSTAT = 1024, NA_CTL = 1088, NA_VIS = 1152, NA_SPTR = 1184;
+
+std::mutex g_na_mu;
+void* g_na_base[64] = {};
+
+// device address of the static scratch on the current device (looked up once per device)
+// error text without heap allocation: the thread's message buffer is reserved during set-up
+void na_error(const char* fmt, const char* a = "", long long x = 0, long long y = 0) {
+    char buf[200];
+    snprintf(buf, sizeof(buf), fmt, a, x, y);
+    t_err.assign(buf);
+}
+
+unsigned char* na_base() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) { na_error("no current device%s"); return nullptr; }
+    std::lock_guard<std::mutex> g(g_na_mu);
+    if (!g_na_base[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, pcbg_noalloc_scratch);
+        if (e != cudaSuccess || !p) { na_error("cudaGetSymbolAddress: %s", cudaGetErrorString(e)); return nullptr; }
+        g_na_base[dev] = p;
+    }
+    return static_cast<unsigned char*>(g_na_base[dev]);
+}
+
+template <typename DT>
+int na_run(pcbg_search* q, unsigned char* base, cudaStream_t stream) {
+    SDev S;
+    memset(&S, 0, sizeof(S));
+    S.rw = q->rw; S.rh = q->rh; S.nl = q->nl; S.pitch = q->pitch; S.hpad = q->hpad;
+    S.ntx = q->pitch / TILE; S.nty = q->hpad / TILE;
+    for (int l = 0; l < MAX_LAYERS; ++l) {
+        float mf = 0.f;
+        for (int d = 0; d < 8; ++d) { S.fac[l][d] = q->fac[l][d]; if (l < q->nl) mf = std::max(mf, q->fac[l][d]); }
+        S.maxfac[l] = mf;
+    }
+    classify(S);
+    if (sizeof(DT) != 4) S.mode = 0;
+    S.cf = q->cf; S.fl = q->flags; S.vcf = q->vcf; S.out = q->out;
+    const size_t states = size_t(q->nl) * q->hpad * q->pitch, tiles = size_t(S.ntx) * S.nty;
+    unsigned char* small = base + NA_DIST + NA_STAMP + NA_WL;
+    S.dist = base;
+    S.stamp = reinterpret_cast<uint32_t*>(base + NA_DIST);
+    SStat st0;
+    st0.ub = ~0ull; st0.maxw = 0; st0.best = ~0ull; st0.maxd = 0; st0.need_wide = 0; st0.pad = 0;
+    const void* sptr[2] = {q->start_idx, q->start_d};
+    const int ns = q->n_starts;
+    cudaMemcpyAsync(small + NA_SDEV, &S, sizeof(S), cudaMemcpyHostToDevice, stream);
+    cudaMemcpyAsync(small + NA_SSTAT, &st0, sizeof(st0), cudaMemcpyHostToDevice, stream);
+    cudaMemcpyAsync(small + NA_SPTR, sptr, sizeof(sptr), cudaMemcpyHostToDevice, stream);
+    cudaMemcpyAsync(small + NA_SPTR + 16, &ns, sizeof(ns), cudaMemcpyHostToDevice, stream);
+    // the array keeps the previous call's contents: clear what must start unreached / zero
+    cudaMemsetAsync(base, 0x7F, states * sizeof(DT), stream);
+    cudaMemsetAsync(base + NA_DIST, 0, tiles * 4, stream);
+    cudaMemsetAsync(small + NA_CTL, 0, C_N * 4, stream);
+    cudaMemsetAsync(small + NA_VIS, 0, 24, stream);
+    SolveArgs a;
+    a.S = reinterpret_cast<const SDev*>(small + NA_SDEV);
+    a.st = reinterpret_cast<SStat*>(small + NA_SSTAT);
+    a.n = 1;
+    a.nlmax = q->nl;
+    a.kmax = S.mode ? S.K : 0;
+    a.wl = reinterpret_cast<unsigned long long*>(base + NA_DIST + NA_STAMP);
+    a.cap = unsigned(tiles);
+    a.ctl = reinterpret_cast<unsigned int*>(small + NA_CTL);
+    a.visits = reinterpret_cast<unsigned long long*>(small + NA_VIS);
+    a.max_rounds = 1 << 20;
+    seed_kernel<DT><<<1, 128, 0, stream>>>(a, reinterpret_cast<const uint32_t* const*>(small + NA_SPTR),
+                                          reinterpret_cast<const uint64_t* const*>(small + NA_SPTR + 8),
+                                          reinterpret_cast<const int*>(small + NA_SPTR + 16));
+    const size_t smem = S.mode ? layout(q->nl, S.K, 4).total : layout(q->nl, 1, sizeof(DT)).total;
+    const int blocks = occupancy_blocks<DT>(smem);
+    if (blocks <= 0) { na_error("relax kernel cannot be resident%s"); return -1; }
+    void* args[] = {&a};
+    cudaError_t e = cudaLaunchCooperativeKernel(reinterpret_cast<void*>(relax_kernel<DT>), dim3(blocks), dim3(NT), args, smem, stream);
+    if (e != cudaSuccess) { na_error("cooperative launch: %s", cudaGetErrorString(e)); return -1; }
+    report_kernel<DT><<<dim3(32, 1), 256, 0, stream>>>(a.S, a.st);
+    SStat x;
+    unsigned int ctl[C_N];
+    cudaMemcpyAsync(&x, small + NA_SSTAT, sizeof(x), cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(ctl, small + NA_CTL, sizeof(ctl), cudaMemcpyDeviceToHost, stream);
+    e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) { na_error("no-alloc solve: %s", cudaGetErrorString(e)); return -1; }
+    if (ctl[C_ERR]) { na_error("no-alloc solve aborted (error bits %s%lld)", "", (long long)ctl[C_ERR]); return -1; }
+    const unsigned long long INF = static_cast<unsigned long long>(Lim<DT>::INF);
+    const bool have = x.ub < INF;
+    q->best = have && x.best != ~0ull ? int64_t(x.best) : -1;
+    q->best_d = have ? x.ub : INF64;
+    q->rounds = int(ctl[C_ROUNDS]);
+    bool redo = false;
+    if (sizeof(DT) == 4) {
+        if (x.need_wide && (!have || x.ub >= static_cast<unsigned long long>(WLIM32))) redo = true;
+        if (!have && x.maxd + x.maxw >= INF) redo = true;
+    }
+    q->status = redo ? 1 : 0;
+    return 0;
+}
+
+}  // namespace
+}  // namespace pcbg
+
+extern "C" int pcbg_solve_noalloc(pcbg_search* s, void* stream) {
+    using namespace pcbg;
+    if (t_err.capacity() < 256) t_err.reserve(256);  // set-up, first call on this thread
+    if (!s || s->nl < 1 || s->nl > MAX_LAYERS || s->rw < 1 || s->rh < 1 || s->pitch % TILE || s->hpad % TILE ||
+        s->pitch < s->rw || s->hpad < s->rh) {
+        na_error("bad search geometry%s");
+        return PCBG_ERR_FAIL;
+    }
+    const size_t states = size_t(s->nl) * s->hpad * s->pitch;
+    if (states > size_t(PCBG_NOALLOC_MAX_STATES)) {
+        na_error("search of %s%lld padded states exceeds the no-alloc limit of %lld states", "", (long long)states,
+                 (long long)PCBG_NOALLOC_MAX_STATES);
+        return PCBG_ERR_FAIL;
+    }
+    unsigned char* base = na_base();
+    if (!base) return PCBG_ERR_FAIL;
+    std::lock_guard<std::mutex> g(g_mu);  // one solve at a time in this process: calls share the array
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (na_run<uint32_t>(s, base, st) != 0) return PCBG_ERR_FAIL;
+    if (s->status == 1) {
+        if (na_run<uint64_t>(s, base, st) != 0) return PCBG_ERR_FAIL;
+        s->status = 1;
+    }
+    return 0;
+}
