@@ -237,6 +237,9 @@ static void solve_rect(const pcbg_query* q, int rx0, int ry0, int rw, int rh, fl
 
 static double dmax3(double a, double b, double c) { double m = a > b ? a : b; return m > c ? m : c; }
 
+static size_t g_max_states = (size_t)48 << 20;
+void pcbo_set_max_states(size_t n) { if (n) g_max_states = n; }
+
 int pcbo_solve(const pcbg_query* q, pcbg_result* out) {
     const size_t FWN = (size_t)q->ww * q->wh, WS = FWN * (size_t)q->nl, WB = WS / 64 + 1;
     int sx0 = 1 << 30, sy0 = 1 << 30, sx1 = -1, sy1 = -1, tx0 = 1 << 30, ty0 = 1 << 30, tx1 = -1, ty1 = -1;
@@ -282,6 +285,8 @@ int pcbo_solve(const pcbg_query* q, pcbg_result* out) {
         }
         const int full = rx0 == 0 && ry0 == 0 && rx1 == q->ww && ry1 == q->wh;
         free(field);
+        field = NULL;
+        if ((size_t)(rx1 - rx0) * (size_t)(ry1 - ry0) * (size_t)q->nl > g_max_states) return -1;
         int64_t best;
         float ub;
         solve_rect(q, rx0, ry0, rx1 - rx0, ry1 - ry0, &field, &best, &ub);

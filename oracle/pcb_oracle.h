@@ -56,6 +56,9 @@ void pcbo_report(int64_t n, const uint64_t* dist, int64_t best, uint64_t best_d,
  * or -1 (no starts or no targets). */
 int pcbo_solve(const pcbg_query* q, pcbg_result* out);
 void pcbo_free(float* p);
+/* The state cap of one rectangle (gpu_configure's max_states; 0: none). A rectangle over it makes pcbo_solve
+ * return -1, as the back end does (src/gpu.cu:426). */
+void pcbo_set_max_states(size_t n);
 
 /* A resolved dense search for the multi-search CPU baseline. */
 typedef struct pcbo_search {

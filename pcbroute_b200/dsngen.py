@@ -1,0 +1,215 @@
+"""Seeded Specctra DSN boards in the grammar pcbroute reads (src/dsn.cpp:75-384).
+
+Boards are deterministic functions of (config, seed). Footprints are built from their published pad geometry:
+- SOIC-8: 8 pads 0.6 x 1.55 mm, 1.27 mm pitch, rows 5.4 mm apart;
+- 0805 / 0603 / 0402: 2 pads, 1.0 x 1.3 / 0.8 x 0.9 / 0.5 x 0.55 mm at 1.9 / 1.6 / 1.0 mm centres;
+- QFP-100: 25 pads per side, 0.3 x 1.5 mm, 0.5 mm pitch, 15.4 mm across the pad rows;
+- BGA-256: 16 x 16 balls of 0.5 mm, 1.0 mm pitch.
+Vias are through-hole (one circle per copper layer). Parts are placed at random without overlapping (with a
+courtyard margin); nets take random pins; classes and planes follow the configuration.
+
+    python -m pcbroute_b200.dsngen c1 1 board.dsn
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+import random
+import sys
+
+
+@dataclasses.dataclass
+class Footprint:
+    name: str
+    pads: list          # (pin id, x um, y um, padstack)
+    w: float            # courtyard
+    h: float
+
+
+def _soic8():
+    pads = []
+    for k in range(4):
+        pads.append((str(k + 1), -2700, -1905 + 1270 * k, "SOIC"))
+        pads.append((str(8 - k), 2700, -1905 + 1270 * k, "SOIC"))
+    return Footprint("SOIC8", pads, 7400, 5600)
+
+
+def _chip(name, dx, stack, w, h):
+    return Footprint(name, [("1", -dx, 0, stack), ("2", dx, 0, stack)], w, h)
+
+
+def _qfp100():
+    pads = []
+    n = 1
+    for side in range(4):
+        for k in range(25):
+            t = -6000 + 500 * k
+            x, y, st = [(-7700, t, "QFPV"), (t, 7700, "QFPH"), (7700, -t, "QFPV"), (-t, -7700, "QFPH")][side]
+            pads.append((str(n), x, y, st))
+            n += 1
+    return Footprint("QFP100", pads, 17500, 17500)
+
+
+def _bga256():
+    pads = []
+    for r in range(16):
+        for c in range(16):
+            pads.append((f"{chr(65 + r)}{c + 1}", -7500 + 1000 * c, -7500 + 1000 * r, "BALL"))
+    return Footprint("BGA256", pads, 18000, 18000)
+
+
+PADSTACKS = {
+    "SOIC": ("rect", -300, -775, 300, 775),
+    "C0805": ("rect", -500, -650, 500, 650),
+    "C0603": ("rect", -400, -450, 400, 450),
+    "C0402": ("rect", -250, -275, 250, 275),
+    "QFPV": ("rect", -750, -150, 750, 150),
+    "QFPH": ("rect", -150, -750, 150, 750),
+    "BALL": ("circle", 500),
+}
+
+FOOTPRINTS = {
+    "SOIC8": _soic8(),
+    "R0805": _chip("R0805", 950, "C0805", 3200, 1900),
+    "R0603": _chip("R0603", 800, "C0603", 2600, 1500),
+    "R0402": _chip("R0402", 500, "C0402", 1800, 1000),
+    "QFP100": _qfp100(),
+    "BGA256": _bga256(),
+}
+
+
+@dataclasses.dataclass
+class Config:
+    name: str
+    w_mm: float
+    h_mm: float
+    layers: list
+    parts: list                  # (footprint, count)
+    nets: int
+    connections: int
+    multipin_frac: float = 0.0   # share of nets with more than 2 pins
+    fanout: tuple = (2, 2)       # pins per multi-pin net
+    classes: list = dataclasses.field(default_factory=lambda: [("default", 250, 200, 1.0)])  # name, width, clr, share
+    planes: list = dataclasses.field(default_factory=list)   # (net, layer)
+
+
+CONFIGS = {
+    # 2 layers, 12 parts (SOIC-8 / 0805), 40 nets, ~60 two-pin connections, one class 250/200 um
+    "c1": Config("c1", 50, 40, ["F.Cu", "B.Cu"], [("SOIC8", 10), ("R0805", 2)], 40, 60),
+    # 4 layers with GND / VCC planes, QFP-100 + 40 0402/0603, 300 nets, 500 connections, 20 % multi-pin (2-6)
+    "c2": Config("c2", 100, 80, ["F.Cu", "In1.Cu", "In2.Cu", "B.Cu"],
+                 [("QFP100", 1), ("R0402", 20), ("R0603", 20), ("SOIC8", 12)], 300, 500, 0.2, (3, 6),
+                 [("default", 200, 150, 0.85), ("power", 400, 250, 0.15)], [("GND", "In1.Cu"), ("VCC", "In2.Cu")]),
+    # small boards for the parity tests
+    "t1": Config("t1", 24, 18, ["F.Cu", "B.Cu"], [("SOIC8", 3), ("R0805", 4)], 10, 14),
+    "t2": Config("t2", 30, 24, ["F.Cu", "In1.Cu", "In2.Cu", "B.Cu"], [("SOIC8", 4), ("R0603", 6)], 16, 24, 0.2, (3, 4),
+                 [("default", 200, 150, 0.8), ("power", 400, 250, 0.2)]),
+}
+
+
+def _place(rng, cfg):
+    W, H = cfg.w_mm * 1000, cfg.h_mm * 1000
+    placed = []
+    for fp_name, count in cfg.parts:
+        fp = FOOTPRINTS[fp_name]
+        for _ in range(count):
+            for _attempt in range(2000):
+                rot = rng.choice([0, 90])
+                w, h = (fp.w, fp.h) if rot == 0 else (fp.h, fp.w)
+                x = rng.uniform(w / 2 + 1500, W - w / 2 - 1500)
+                y = rng.uniform(h / 2 + 1500, H - h / 2 - 1500)
+                if not any(abs(x - px) * 2 < w + pw + 600 and abs(y - py) * 2 < h + ph + 600
+                           for (_, _, px, py, pw, ph, _) in placed):
+                    placed.append((fp_name, f"{fp_name[0]}{len(placed) + 1}", round(x), round(y), w, h, rot))
+                    break
+    return placed
+
+
+def generate(config: str, seed: int) -> str:
+    cfg = CONFIGS[config]
+    rng = random.Random(f"{config}:{seed}")
+    placed = _place(rng, cfg)
+    pins = [f"{ref}-{pid}" for (fp, ref, *_rest) in placed for (pid, *_p) in FOOTPRINTS[fp].pads]
+    rng.shuffle(pins)
+    nets = []
+    # plane nets take a handful of pins each
+    for net, _layer in cfg.planes:
+        k = min(len(pins), rng.randint(4, 8))
+        nets.append((net, [pins.pop() for _ in range(k)]))
+    conns = 0
+    i = 0
+    while len(nets) < cfg.nets + len(cfg.planes) and len(pins) >= 2 and conns < cfg.connections:
+        multi = rng.random() < cfg.multipin_frac
+        k = rng.randint(*cfg.fanout) if multi else 2
+        k = min(k, len(pins), cfg.connections - conns + 1)
+        if k < 2:
+            break
+        nets.append((f"N{i}", [pins.pop() for _ in range(k)]))
+        conns += k - 1
+        i += 1
+    # classes: a share of the signal nets each
+    names = [n for n, _ in nets]
+    cls_of = {}
+    shares = [c[3] for c in cfg.classes]
+    for n in names:
+        r, acc = rng.random(), 0.0
+        for c, s in zip(cfg.classes, shares):
+            acc += s
+            if r <= acc:
+                cls_of[n] = c[0]
+                break
+        else:
+            cls_of[n] = cfg.classes[0][0]
+    W, H = round(cfg.w_mm * 1000), round(cfg.h_mm * 1000)
+    L = []
+    L.append(f"(pcb {config}_{seed}.dsn")
+    L.append("  (resolution um 10)")
+    L.append("  (unit um)")
+    L.append("  (structure")
+    for ly in cfg.layers:
+        L.append(f"    (layer {ly} (type signal))")
+    L.append(f"    (boundary (path pcb 0  0 0  {W} 0  {W} {H}  0 {H}  0 0))")
+    for net, layer in cfg.planes:
+        L.append(f"    (plane {net} (polygon {layer} 0  500 500  {W - 500} 500  {W - 500} {H - 500}  500 {H - 500}))")
+    L.append("    (via V)")
+    d0, w0, c0, _ = cfg.classes[0]
+    L.append(f"    (rule (width {w0}) (clearance {c0}))")
+    L.append("  )")
+    L.append("  (placement")
+    by_fp = {}
+    for fp, ref, x, y, _w, _h, rot in placed:
+        by_fp.setdefault(fp, []).append(f"(place {ref} {x} {y} front {rot})")
+    for fp, pl in by_fp.items():
+        L.append(f"    (component {fp} " + " ".join(pl) + ")")
+    L.append("  )")
+    L.append("  (library")
+    for fp in by_fp:
+        f = FOOTPRINTS[fp]
+        L.append(f"    (image {fp} " + " ".join(f"(pin {st} {pid} {x} {y})" for pid, x, y, st in f.pads) + ")")
+    used = sorted({st for fp in by_fp for (_, _, _, st) in FOOTPRINTS[fp].pads})
+    for st in used:
+        s = PADSTACKS[st]
+        shape = f"(rect F.Cu {s[1]} {s[2]} {s[3]} {s[4]})" if s[0] == "rect" else f"(circle F.Cu {s[1]})"
+        L.append(f"    (padstack {st} (shape {shape}) (attach off))")
+    L.append("    (padstack V " + " ".join(f"(shape (circle {ly} 600))" for ly in cfg.layers) + " (attach off))")
+    L.append("  )")
+    L.append("  (network")
+    for n, ps in nets:
+        L.append(f"    (net {n} (pins {' '.join(ps)}))")
+    for cname, cw, cc, _ in cfg.classes:
+        members = [n for n in names if cls_of[n] == cname]
+        if members:
+            L.append(f"    (class {cname} {' '.join(members)} (circuit (use_via V)) (rule (width {cw}) (clearance {cc})))")
+    L.append("  )")
+    L.append(")")
+    return "\n".join(L) + "\n"
+
+
+def main() -> None:
+    config, seed, path = sys.argv[1], int(sys.argv[2]), sys.argv[3]
+    with open(path, "w") as f:
+        f.write(generate(config, seed))
+
+
+if __name__ == "__main__":
+    main()
