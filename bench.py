@@ -105,6 +105,27 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def cost_map_roofline(lib, peak):
+    """Device rebuild of the congestion cost maps (rebuild_costs, src/router.cpp:409-420) on a board the size of the
+    8-layer stress configuration: 5000 x 4000 cells, 8 layers, 4 net classes. Algorithmic bytes per rebuild: per
+    class and layer st 2 + oc 1 + cst 4 per cell; per class vst 2 + 8 ov + vcst 4 per cell; the 8 history planes
+    (4 B) once."""
+    nx, ny, nl, k = 5000, 4000, 8, 4
+    h = lib.pcbg_costs_create(nx, ny, nl, k)
+    if not h:
+        return None
+    try:
+        ms = lib.pcbg_costs_time_rebuild(h, 2.5, 0, 10)
+    finally:
+        lib.pcbg_costs_destroy(h)
+    n = nx * ny
+    alg = k * (nl * n * 7 + n * (2 + nl + 4)) + nl * n * 4
+    ach = alg / (ms / 1e3) / 1e9
+    return {"kernel": "costs_rebuild_kernel", "workload": "5000 x 4000 cells, 8 layers, 4 classes",
+            "ms": round(ms, 3), "bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(ach / peak, 4), "algorithmic_bytes": alg}
+
+
 def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -384,6 +405,7 @@ def main():
                          "kernel_ms_per_step": round(kms / args.steps, 3), "peak_kind": peak_kind},
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
+            "cost_maps": cost_map_roofline(lib, peak),
             "e2e": e2e,
             "cpu_baseline": cpu,
         }

@@ -155,6 +155,36 @@ float pcbg_last_batch_kernel_ms(void);
 int32_t pcbg_last_batch_launches(void);
 int64_t pcbg_last_batch_local_iters(void);   /* sum over tile visits of local relaxation iterations */
 
+/* ---- device-resident congestion cost maps (src/router.cpp:197-211, 383-420, 1880-1999) ---------------------- */
+
+/* The cost maps the searches read, kept in HBM and updated in place: per class k, the static owner grids st[l] / vst
+ * (0 free, 0xFFFF blocked, else the owning net + 1), the other nets' occupancy oc[l] / ov[l] (u8 counts), the
+ * history hist[l] (shared by the classes) and an optional ground-pour factor per layer; outputs cst[l] / vcst
+ * (RClass::cst / vcst). All host arrays are layer-major [l][j * nx + i]. */
+typedef struct pcbg_costs pcbg_costs;
+pcbg_costs* pcbg_costs_create(int32_t nx, int32_t ny, int32_t nl, int32_t nclasses);
+void pcbg_costs_destroy(pcbg_costs* h);
+int pcbg_costs_set_static(pcbg_costs* h, int32_t cls, const uint16_t* st, const uint16_t* vst);
+int pcbg_costs_set_occupancy(pcbg_costs* h, int32_t cls, const uint8_t* oc, const uint8_t* ov);
+int pcbg_costs_set_history(pcbg_costs* h, const float* hist);
+int pcbg_costs_set_ground(pcbg_costs* h, int32_t layer, const float* fac);   /* NULL: none on that layer */
+/* rebuild_costs(pres, hard) (src/router.cpp:409-420): every cost of every class. */
+int pcbg_costs_rebuild(pcbg_costs* h, float pres, int32_t hard);
+/* A commit's stamp of one grid (class cls, kind 0 track / 1 via, layer): occupancy +1 (sign > 0, saturating at 255)
+ * or -1 over the spans (j, i0, i1 triples, non-overlapping as the router merges them), then the costs of those cells
+ * recomputed with the last rebuild's pres / hard (stamp + refresh_costs, src/router.cpp:1880-1963). */
+int pcbg_costs_stamp(pcbg_costs* h, int32_t cls, int32_t kind, int32_t layer, const int32_t* spans, int32_t nspans,
+                     int32_t sign);
+/* count_conflicts(mark_hist) (src/router.cpp:1970-1999): hist += inc at the listed states l * nx * ny + cell, in
+ * list order. */
+int pcbg_costs_add_history(pcbg_costs* h, const uint32_t* states, int32_t m, float inc);
+int pcbg_costs_download(pcbg_costs* h, int32_t cls, float* cst, float* vcst);
+int pcbg_costs_download_history(pcbg_costs* h, float* hist);
+/* Device pointer of a class's map (layer -1: the via map), for searches that read costs in place. */
+const float* pcbg_costs_device_map(pcbg_costs* h, int32_t cls, int32_t layer);
+/* Mean device time (ms, CUDA events) of `reps` full rebuilds. */
+float pcbg_costs_time_rebuild(pcbg_costs* h, float pres, int32_t hard, int32_t reps);
+
 /* ---- seeded synthetic search generator (the batched-search microbenchmark workload) ----------------------- */
 
 /* Fill a pitched search with the seeded workload: per (layer, cell) cost 1 + (h % 16), about 15 % of cells

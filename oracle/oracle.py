@@ -147,3 +147,23 @@ def solve_many(searches: list[dict], threads: int) -> list[tuple[int, int]]:
         a.n_starts, a.start_idx, a.start_d = len(si), si.ctypes.data, sd.ctypes.data
     lib().pcbo_solve_many(arr, len(searches), threads)
     return [(int(arr[k].best), int(arr[k].best_d)) for k in range(len(searches))]
+
+
+def costs_rebuild(st, oc, ov, vst, hist, gnd, pres: float, hard: bool):
+    """Cost maps of every class (src/router.cpp:386-405): st/oc/ov [k, l, n], vst [k, n], hist [l, n],
+    gnd: list per layer of [n] float32 or None. Returns cst [k, l, n], vcst [k, n]."""
+    k, nl, n = st.shape
+    L = lib()
+    L.pcbo_costs_rebuild.argtypes = [C.c_int] * 3 + [C.c_void_p] * 6 + [C.c_float, C.c_int, C.c_void_p, C.c_void_p]
+    st = np.ascontiguousarray(st, np.uint16)
+    oc = np.ascontiguousarray(oc, np.uint8)
+    ov = np.ascontiguousarray(ov, np.uint8)
+    vst = np.ascontiguousarray(vst, np.uint16)
+    hist = np.ascontiguousarray(hist, np.float32)
+    gk = [None if g is None else np.ascontiguousarray(g, np.float32) for g in (gnd or [None] * nl)]
+    gp = (C.c_void_p * nl)(*[None if g is None else g.ctypes.data for g in gk])
+    cst = np.empty((k, nl, n), np.float32)
+    vcst = np.empty((k, n), np.float32)
+    L.pcbo_costs_rebuild(n, nl, k, st.ctypes.data, oc.ctypes.data, ov.ctypes.data, vst.ctypes.data, hist.ctypes.data,
+                         C.cast(gp, C.c_void_p), pres, 1 if hard else 0, cst.ctypes.data, vcst.ctypes.data)
+    return cst, vcst

@@ -348,3 +348,48 @@ void pcbo_solve_many(pcbo_search* s, int n, int threads) {
     for (int t = 0; t < threads; ++t) pthread_join(th[t], NULL);
     free(th);
 }
+
+/* ---- congestion cost maps: cost_xp / vcost_xp with own = 0 (src/router.cpp:386-405), over whole grids ---- */
+
+void pcbo_costs_rebuild(int n, int nl, int nclasses, const uint16_t* st, const uint8_t* oc, const uint8_t* ov,
+                        const uint16_t* vst, const float* hist, const float* const* gnd, float pres, int hard,
+                        float* cst, float* vcst) {
+    for (int k = 0; k < nclasses; ++k) {
+        for (int l = 0; l < nl; ++l)
+            for (int c = 0; c < n; ++c) {
+                const size_t id = ((size_t)k * nl + l) * n + c;
+                const uint16_t s = st[id];
+                float v;
+                if (s == 0xFFFF) v = CINF;
+                else {
+                    const int occ = oc[id];
+                    if (hard && occ > 0) v = CINF;
+                    else {
+                        v = (1.f + hist[(size_t)l * n + c]) * (1.f + pres * (float)(occ > 0 ? occ : 0));
+                        if (gnd && gnd[l]) v *= gnd[l][c];
+                        if (s != 0) v = -v;
+                    }
+                }
+                cst[id] = v;
+            }
+        for (int c = 0; c < n; ++c) {
+            const uint16_t s = vst[(size_t)k * n + c];
+            float v;
+            if (s == 0xFFFF) v = CINF;
+            else {
+                int occ = 0;
+                float hs = 0;
+                for (int l = 0; l < nl; ++l) {
+                    occ += ov[((size_t)k * nl + l) * n + c];
+                    hs += hist[(size_t)l * n + c];
+                }
+                if (hard && occ > 0) v = CINF;
+                else {
+                    v = (1.f + hs / (float)nl) * (1.f + pres * (float)(occ > 0 ? occ : 0));
+                    if (s != 0) v = -v;
+                }
+            }
+            vcst[(size_t)k * n + c] = v;
+        }
+    }
+}

@@ -60,6 +60,13 @@ void pcbo_free(float* p);
  * return -1, as the back end does (src/gpu.cu:426). */
 void pcbo_set_max_states(size_t n);
 
+/* The congestion cost maps of every class (src/router.cpp:386-405 with own = 0; rebuild_costs 409-420):
+ * st/oc/ov [k][l][n], vst [k][n], hist [l][n], gnd[l] (NULL entries or NULL: no ground factor);
+ * outputs cst [k][l][n], vcst [k][n]. */
+void pcbo_costs_rebuild(int n, int nl, int nclasses, const uint16_t* st, const uint8_t* oc, const uint8_t* ov,
+                        const uint16_t* vst, const float* hist, const float* const* gnd, float pres, int hard,
+                        float* cst, float* vcst);
+
 /* A resolved dense search for the multi-search CPU baseline. */
 typedef struct pcbo_search {
     int rw, rh, nl;

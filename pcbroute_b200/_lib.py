@@ -16,7 +16,11 @@ LIB_PATH = _build.LIB
 PCBG_SYMBOLS = [
     "pcbg_available", "pcbg_configure", "pcbg_solve", "pcbg_host_acquire", "pcbg_host_release", "pcbg_last_error",
     "pcbg_solve_batch", "pcbg_solve_noalloc", "pcbg_last_batch_tile_visits", "pcbg_last_batch_layer_visits", "pcbg_last_batch_rounds",
-    "pcbg_last_batch_kernel_ms", "pcbg_last_batch_launches", "pcbg_last_batch_local_iters", "pcbg_synth_search", "pcbg_synth_search_host",
+    "pcbg_last_batch_kernel_ms", "pcbg_last_batch_launches", "pcbg_last_batch_local_iters", "pcbg_synth_search",
+    "pcbg_synth_search_host", "pcbg_costs_create", "pcbg_costs_destroy", "pcbg_costs_set_static",
+    "pcbg_costs_set_occupancy", "pcbg_costs_set_history", "pcbg_costs_set_ground", "pcbg_costs_rebuild",
+    "pcbg_costs_stamp", "pcbg_costs_add_history", "pcbg_costs_download", "pcbg_costs_download_history",
+    "pcbg_costs_device_map", "pcbg_costs_time_rebuild",
 ]
 GPU_H_SYMBOLS = [
     "_Z13gpu_availablev",                        # bool gpu_available()
@@ -113,6 +117,23 @@ def load() -> C.CDLL:
     lib.pcbg_synth_search.argtypes = [C.c_uint64, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_float,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.pcbg_synth_search.restype = C.c_int
+    V = C.c_void_p
+    lib.pcbg_costs_create.argtypes = [C.c_int32] * 4
+    lib.pcbg_costs_create.restype = V
+    lib.pcbg_costs_destroy.argtypes = [V]
+    lib.pcbg_costs_set_static.argtypes = [V, C.c_int32, V, V]
+    lib.pcbg_costs_set_occupancy.argtypes = [V, C.c_int32, V, V]
+    lib.pcbg_costs_set_history.argtypes = [V, V]
+    lib.pcbg_costs_set_ground.argtypes = [V, C.c_int32, V]
+    lib.pcbg_costs_rebuild.argtypes = [V, C.c_float, C.c_int32]
+    lib.pcbg_costs_stamp.argtypes = [V, C.c_int32, C.c_int32, C.c_int32, V, C.c_int32, C.c_int32]
+    lib.pcbg_costs_add_history.argtypes = [V, V, C.c_int32, C.c_float]
+    lib.pcbg_costs_download.argtypes = [V, C.c_int32, V, V]
+    lib.pcbg_costs_download_history.argtypes = [V, V]
+    lib.pcbg_costs_device_map.argtypes = [V, C.c_int32, C.c_int32]
+    lib.pcbg_costs_device_map.restype = V
+    lib.pcbg_costs_time_rebuild.argtypes = [V, C.c_float, C.c_int32, C.c_int32]
+    lib.pcbg_costs_time_rebuild.restype = C.c_float
     _lib = lib
     return lib
 
