@@ -37,6 +37,7 @@ struct SDev {
     const float* vcf;
     void* dist;
     uint32_t* stamp;
+    uint32_t* sides;   // per tile: which halo sides changed since its last visit (bit 8: everything)
     float* out;
 };
 

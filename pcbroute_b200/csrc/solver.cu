@@ -92,11 +92,13 @@ struct SolveArgs {
 struct Lay {
     size_t d, w, v, e, m, total;
 };
-__host__ __device__ inline Lay layout(int nlm, int planes, size_t dsz) {
+// wbytes: bytes per state of the w region (joint: K u16 planes, at least one float plane for the fallback)
+__host__ __device__ inline int joint_wbytes(int K) { return 2 * K > 4 ? 2 * K : 4; }
+__host__ __device__ inline Lay layout(int nlm, int wbytes, size_t dsz) {
     Lay L;
     size_t o = 0;
     L.d = o; o += size_t(nlm) * LS * dsz; o = (o + 15) & ~size_t(15);
-    L.w = o; o += size_t(planes) * nlm * WLS * 4; o = (o + 15) & ~size_t(15);
+    L.w = o; o += size_t(wbytes) * nlm * WLS; o = (o + 15) & ~size_t(15);
     L.v = o; o += size_t(WLS) * dsz; o = (o + 15) & ~size_t(15);
     L.e = o; o += size_t(nlm) * 4 * TILE * dsz; o = (o + 15) & ~size_t(15);
     L.m = o; o += size_t(2) * WLS * 4; o = (o + 15) & ~size_t(15);
@@ -105,7 +107,7 @@ __host__ __device__ inline Lay layout(int nlm, int planes, size_t dsz) {
 }
 __host__ __device__ inline Lay layout_for(int nlm, int kmax, size_t dsz, int mode) {
     // one dynamic allocation serves both modes: the larger of the two layouts, same offsets per mode
-    return mode ? layout(nlm, kmax, 4) : layout(nlm, 1, dsz);
+    return mode ? layout(nlm, joint_wbytes(kmax), 4) : layout(nlm, 4, dsz);
 }
 
 // Software grid barrier with a bounded wait: every block of the cooperative launch is resident, so the wait ends
@@ -143,9 +145,38 @@ __device__ __forceinline__ void enqueue(const SolveArgs& a, const SDev& S, int s
 }
 
 struct VisitShared {
-    unsigned int marks, any, wide, iters;
+    unsigned int marks, any, wide, iters, sides;
     unsigned long long tmin, wmax;
 };
+
+// Halo sides of a tile, as neighbour directions: 0 L, 1 R, 2 T, 3 B, 4 TL, 5 TR, 6 BL, 7 BR; SIDE_ALL: the interior
+// itself changed (a start was written, or the last visit stopped early), every line must be walked.
+constexpr unsigned SIDE_ALL = 1u << 8;
+__device__ __forceinline__ unsigned opposite_side(int b) {
+    const int opp[8] = {1, 0, 3, 2, 7, 6, 5, 4};
+    return 1u << opp[b];
+}
+
+// The lines whose end cells lie on the given halo sides (their first iteration's dirty set), as 6 words (rows,
+// columns, diagonals e + 31 in 2 words, anti-diagonals s in 2 words). A line reads the halo only at its two ends:
+// rows at columns -1 / 32, columns at rows -1 / 32, diagonal e at (e, 0) - (1, 1) and its far end, anti-diagonal s
+// at (s - lo + 1, lo - 1) and (lo - 1, s - lo + 1).
+__device__ __forceinline__ void side_lines(unsigned sides, uint32_t (&w)[6]) {
+    for (int k = 0; k < 6; ++k) w[k] = 0;
+    if (sides & SIDE_ALL) {
+        w[0] = w[1] = w[2] = w[4] = 0xFFFFFFFFu;
+        w[3] = w[5] = 0x7FFFFFFFu;
+        return;
+    }
+    const uint32_t LO = 0xFFFFFFFFu;                         // bits 0..31 of a 63-bit set
+    const uint32_t HI0 = 0x80000000u, HI1 = 0x7FFFFFFFu;     // bits 31..62
+    if (sides & 1u) { w[0] = LO; w[2] |= LO; w[4] |= LO; }                                // left
+    if (sides & 2u) { w[0] = LO; w[2] |= HI0; w[3] |= HI1; w[4] |= HI0; w[5] |= HI1; }   // right
+    if (sides & 4u) { w[1] = LO; w[2] |= HI0; w[3] |= HI1; w[4] |= LO; }                 // top
+    if (sides & 8u) { w[1] = LO; w[2] |= LO; w[4] |= HI0; w[5] |= HI1; }                 // bottom
+    if (sides & (16u | 128u)) w[2] |= HI0;                                               // corners TL, BR: diagonal 0
+    if (sides & (32u | 64u)) w[4] |= HI0;                                                // corners TR, BL: anti-diagonal 31
+}
 
 // ---- staging shared by both modes ----
 
@@ -156,7 +187,8 @@ __device__ void stage_dist(const SDev& S, DT* dS, int x0, int y0) {
         const int l = idx / (HS * HS), rem = idx % (HS * HS), r = rem / HS, c = rem % HS;
         const int gy = y0 + r - 1, gx = x0 + c - 1;
         DT v = Lim<DT>::INF;
-        if (gy >= 0 && gy < S.hpad && gx >= 0 && gx < S.pitch) v = dist[(size_t(l) * S.hpad + gy) * S.pitch + gx];
+        // distances are written by other blocks during the launch: read them at L2, never from this SM's L1
+        if (gy >= 0 && gy < S.hpad && gx >= 0 && gx < S.pitch) v = __ldcg(dist + (size_t(l) * S.hpad + gy) * S.pitch + gx);
         dS[l * LS + r * DSTR + c] = v;
     }
 }
@@ -208,95 +240,193 @@ __device__ void save_edges(const SDev& S, const DT* dS, DT* eS) {
 
 // One cell of a line: every layer's move from the previous cell of the line, then vias among the layers.
 template <int NL>
-__device__ __forceinline__ void jstep(uint32_t* dS, const uint32_t* wP, const uint32_t* vS, const uint32_t* vokS,
+__device__ __forceinline__ void jstep(uint32_t* dS, const uint16_t* wP, const uint32_t* vS, const uint32_t* vokS,
                                       int dofs, int wofs, uint32_t (&prev)[NL], int& ch) {
     uint32_t v[NL], c[NL];
     uint32_t m = INF32;
     #pragma unroll
     for (int l = 0; l < NL; ++l) {
         v[l] = dS[l * LS + dofs];
-        c[l] = min(v[l], prev[l] + wP[l * WLS + wofs]);
+        const uint32_t w16 = wP[l * WLS + wofs];
+        c[l] = min(v[l], prev[l] + (w16 == 0xFFFFu ? INF32 : w16));   // 0xFFFF: impassable
         m = min(m, c[l]);
     }
     const uint32_t mv = m + vS[wofs];
     const uint32_t vm = vokS[wofs];
+    uint32_t any = 0;
     #pragma unroll
     for (int l = 0; l < NL; ++l) {
-        if ((vm >> l) & 1u) c[l] = min(c[l], mv);
-        if (c[l] < v[l]) { atomicMin(dS + l * LS + dofs, c[l]); ch = 1; }
+        c[l] = ((vm >> l) & 1u) ? min(c[l], mv) : c[l];
+        any |= uint32_t(c[l] < v[l]);
+        atomicMin(dS + l * LS + dofs, c[l]);   // unconditional: no branch; a min that lowers nothing is harmless
         prev[l] = c[l];
     }
+    ch = int(any);
 }
 
+// A line of the tile walked forward then backward: cell k at distance offset d0 + k * ds and weight offset
+// w0 + k * ws, k < len; pf / pb: the halo cells before the first / after the last cell. One call site per thread
+// and no unrolling: the walk is inlined once per layer count, which keeps the kernel in the instruction cache.
+// Returns the positions k at which any layer's cost went down.
 template <int NL>
-__device__ int joint_pass(const SDev& S, uint32_t* dS, const uint32_t* wS, const uint32_t* vS, const uint32_t* vokS) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int ch = 0;
+__device__ __forceinline__ uint32_t walk_line(uint32_t* dS, const uint16_t* wP, const uint32_t* vS, const uint32_t* vokS,
+                                              int d0, int ds, int w0, int ws, int len, int pf, int pb) {
+    uint32_t moved = 0;
+    int ch;
     uint32_t prev[NL];
-    if (warp == 0) {            // rows: +x then -x
-        const uint32_t* wP = wS + S.plane_h * S.nl * WLS;
-        const int r = lane;
-        #pragma unroll
-        for (int l = 0; l < NL; ++l) prev[l] = dS[l * LS + (r + 1) * DSTR];
-        for (int k = 0; k < TILE; ++k) jstep<NL>(dS, wP, vS, vokS, (r + 1) * DSTR + k + 1, r * CSTR + k, prev, ch);
-        #pragma unroll
-        for (int l = 0; l < NL; ++l) prev[l] = dS[l * LS + (r + 1) * DSTR + TILE + 1];
-        for (int k = TILE - 1; k >= 0; --k) jstep<NL>(dS, wP, vS, vokS, (r + 1) * DSTR + k + 1, r * CSTR + k, prev, ch);
-    } else if (warp == 1) {     // columns: +y then -y
-        const uint32_t* wP = wS + S.plane_v * S.nl * WLS;
-        const int c = lane;
-        #pragma unroll
-        for (int l = 0; l < NL; ++l) prev[l] = dS[l * LS + c + 1];
-        for (int k = 0; k < TILE; ++k) jstep<NL>(dS, wP, vS, vokS, (k + 1) * DSTR + c + 1, k * CSTR + c, prev, ch);
-        #pragma unroll
-        for (int l = 0; l < NL; ++l) prev[l] = dS[l * LS + (TILE + 1) * DSTR + c + 1];
-        for (int k = TILE - 1; k >= 0; --k) jstep<NL>(dS, wP, vS, vokS, (k + 1) * DSTR + c + 1, k * CSTR + c, prev, ch);
-    } else if (warp < 4) {      // main diagonals i - j = e: (+,+) then (-,-)
-        const int e = (warp - 2) * 32 + lane - (TILE - 1);
-        if (e <= TILE - 1) {
-            const uint32_t* wP = wS + S.plane_d * S.nl * WLS;
-            const int i0 = e > 0 ? e : 0, j0 = e < 0 ? -e : 0, len = TILE - (e < 0 ? -e : e);
-            #pragma unroll
-            for (int l = 0; l < NL; ++l) prev[l] = dS[l * LS + j0 * DSTR + i0];
-            for (int k = 0; k < len; ++k)
-                jstep<NL>(dS, wP, vS, vokS, (j0 + k + 1) * DSTR + i0 + k + 1, (j0 + k) * CSTR + i0 + k, prev, ch);
-            #pragma unroll
-            for (int l = 0; l < NL; ++l) prev[l] = dS[l * LS + (j0 + len + 1) * DSTR + i0 + len + 1];
-            for (int k = len - 1; k >= 0; --k)
-                jstep<NL>(dS, wP, vS, vokS, (j0 + k + 1) * DSTR + i0 + k + 1, (j0 + k) * CSTR + i0 + k, prev, ch);
-        }
-    } else if (warp < 6) {      // anti-diagonals i + j = s: (-,+) with j rising, then (+,-) with i rising
-        const int s = (warp - 4) * 32 + lane;
-        if (s <= 2 * TILE - 2) {
-            const uint32_t* wP = wS + S.plane_d * S.nl * WLS;
-            const int lo = s > TILE - 1 ? s - (TILE - 1) : 0;
-            const int len = TILE - (s > TILE - 1 ? s - (TILE - 1) : (TILE - 1) - s);
-            #pragma unroll
-            for (int l = 0; l < NL; ++l) prev[l] = dS[l * LS + lo * DSTR + (s - lo + 2)];
-            for (int k = 0; k < len; ++k) {
-                const int j = lo + k, i = s - j;
-                jstep<NL>(dS, wP, vS, vokS, (j + 1) * DSTR + i + 1, j * CSTR + i, prev, ch);
-            }
-            #pragma unroll
-            for (int l = 0; l < NL; ++l) prev[l] = dS[l * LS + (s - lo + 2) * DSTR + lo];
-            for (int k = 0; k < len; ++k) {
-                const int i = lo + k, j = s - i;
-                jstep<NL>(dS, wP, vS, vokS, (j + 1) * DSTR + i + 1, j * CSTR + i, prev, ch);
-            }
-        }
+    #pragma unroll
+    for (int l = 0; l < NL; ++l) prev[l] = dS[l * LS + pf];
+    for (int k = 0; k < len; ++k) {
+        jstep<NL>(dS, wP, vS, vokS, d0 + k * ds, w0 + k * ws, prev, ch);
+        moved |= uint32_t(ch) << k;
     }
-    return ch;
+    #pragma unroll
+    for (int l = 0; l < NL; ++l) prev[l] = dS[l * LS + pb];
+    for (int k = len - 1; k >= 0; --k) {
+        jstep<NL>(dS, wP, vS, vokS, d0 + k * ds, w0 + k * ws, prev, ch);
+        moved |= uint32_t(ch) << k;
+    }
+    return moved;
 }
 
+// bit k of x to bit 2k (32 -> 64 bits)
+__device__ __forceinline__ uint64_t spread2(uint32_t x) {
+    uint64_t v = x;
+    v = (v | (v << 16)) & 0x0000FFFF0000FFFFull;
+    v = (v | (v << 8)) & 0x00FF00FF00FF00FFull;
+    v = (v | (v << 4)) & 0x0F0F0F0F0F0F0F0Full;
+    v = (v | (v << 2)) & 0x3333333333333333ull;
+    v = (v | (v << 1)) & 0x5555555555555555ull;
+    return v;
+}
+
+// Line ids of a tile: 0-31 rows r, 32-63 columns c, 64-126 main diagonals i - j = e (id 95 + e), 127-189
+// anti-diagonals i + j = s (id 127 + s). Dirty sets are 6 words: rows, columns, 2 x diagonals, 2 x anti-diagonals.
+constexpr int NLINES = 190;
+
+// Walk line `id`, then add to `mark` every line through a cell whose cost went down (its own included).
 template <int NL>
-__device__ int relax_joint(const SDev& S, uint32_t* dS, const uint32_t* wS, const uint32_t* vS, const uint32_t* vokS,
+__device__ __forceinline__ bool walk_id(const SDev& S, uint32_t* dS, const uint16_t* wS, const uint32_t* vS,
+                                        const uint32_t* vokS, int id, uint32_t (&mark)[6]) {
+    int plane, d0, ds, w0, ws, len, pf, pb;
+    int fam, a0 = 0, b0 = 0;
+    if (id < 32) {
+        const int r = id;
+        fam = 0; a0 = r;
+        plane = S.plane_h; d0 = (r + 1) * DSTR + 1; ds = 1; w0 = r * CSTR; ws = 1; len = TILE;
+        pf = (r + 1) * DSTR; pb = (r + 1) * DSTR + TILE + 1;
+    } else if (id < 64) {
+        const int c = id - 32;
+        fam = 1; a0 = c;
+        plane = S.plane_v; d0 = DSTR + c + 1; ds = DSTR; w0 = c; ws = CSTR; len = TILE;
+        pf = c + 1; pb = (TILE + 1) * DSTR + c + 1;
+    } else if (id < 127) {
+        const int e = id - 95;
+        const int i0 = e > 0 ? e : 0, j0 = e < 0 ? -e : 0;
+        fam = 2; a0 = i0; b0 = j0;
+        plane = S.plane_d; len = TILE - (e < 0 ? -e : e);
+        d0 = (j0 + 1) * DSTR + i0 + 1; ds = DSTR + 1; w0 = j0 * CSTR + i0; ws = CSTR + 1;
+        pf = j0 * DSTR + i0; pb = (j0 + len + 1) * DSTR + i0 + len + 1;
+    } else {
+        const int s = id - 127;
+        const int lo = s > TILE - 1 ? s - (TILE - 1) : 0;
+        fam = 3; a0 = s; b0 = lo;
+        plane = S.plane_d; len = TILE - (s > TILE - 1 ? s - (TILE - 1) : (TILE - 1) - s);
+        d0 = (lo + 1) * DSTR + (s - lo) + 1; ds = DSTR - 1; w0 = lo * CSTR + (s - lo); ws = CSTR - 1;
+        pf = lo * DSTR + (s - lo + 2); pb = (s - lo + 2) * DSTR + lo;
+    }
+    const uint32_t M = walk_line<NL>(dS, wS + plane * S.nl * WLS, vS, vokS, d0, ds, w0, ws, len, pf, pb);
+    if (!M) return false;
+    uint64_t d1 = 0, d2 = 0;
+    if (fam == 0) {            // row r, cell (r, k): column k, diagonal k - r, anti-diagonal r + k
+        mark[0] |= 1u << a0;
+        mark[1] |= M;
+        d1 = uint64_t(M) << (TILE - 1 - a0);
+        d2 = uint64_t(M) << a0;
+    } else if (fam == 1) {     // column c, cell (k, c): row k, diagonal c - k, anti-diagonal k + c
+        mark[1] |= 1u << a0;
+        mark[0] |= M;
+        d1 = uint64_t(__brev(M)) << a0;
+        d2 = uint64_t(M) << a0;
+    } else if (fam == 2) {     // diagonal from (i0, j0), cell (j0 + k, i0 + k): anti-diagonal i0 + j0 + 2k
+        const int e = id - 95;
+        d1 = 1ull << (e + TILE - 1);
+        mark[0] |= M << b0;
+        mark[1] |= M << a0;
+        d2 = spread2(M) << (a0 + b0);
+    } else {                   // anti-diagonal s, cell (lo + k, s - lo - k): diagonal s - 2 lo - 2k
+        const int s = a0, lo = b0;
+        d2 = 1ull << s;
+        mark[0] |= M << lo;
+        mark[1] |= __brev(M) >> (TILE - 1 - (s - lo));
+        d1 = spread2(__brev(M)) >> (TILE - 1 - s + 2 * lo);
+    }
+    mark[2] |= uint32_t(d1);
+    mark[3] |= uint32_t(d1 >> 32);
+    mark[4] |= uint32_t(d2);
+    mark[5] |= uint32_t(d2 >> 32);
+    return true;
+}
+
+// Relax a tile to its local fixed point. Every line starts dirty; each iteration walks only the dirty lines, packed
+// onto the fewest warps, and marks the lines through the cells that went down. The visit ends after an iteration
+// with no dirty line, i.e. after a pass in which no line changed anything.
+template <int NL>
+__device__ int relax_joint(const SDev& S, uint32_t* dS, const uint16_t* wS, const uint32_t* vS, const uint32_t* vokS,
                            VisitShared& sh, bool& requeue) {
+    __shared__ uint32_t dirty[2][6];
+    __shared__ uint16_t list[NT];
+    __shared__ int wcount[NT / 32];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) {
+        uint32_t w[6];
+        side_lines(sh.sides, w);
+        for (int k = 0; k < 6; ++k) dirty[0][k] = w[k];
+    }
+    int cur = 0;
     for (int it = 0;; ++it) {
-        const int ch = joint_pass<NL>(S, dS, wS, vS, vokS);
-        const int any = __syncthreads_or(ch);
-        if (!any) return it + 1;
-        if (threadIdx.x == 0) sh.any = 1;
-        if (it + 1 >= MAX_IT) { requeue = true; return it + 1; }
+        if (tid < 6) dirty[cur ^ 1][tid] = 0;
+        __syncthreads();
+        // compact the dirty lines into list[0..total)
+        bool d = false;
+        if (tid < NLINES) {
+            int w, b;
+            if (tid < 64) { w = tid >> 5; b = tid & 31; }
+            else if (tid < 127) { w = 2 + ((tid - 64) >> 5); b = (tid - 64) & 31; }
+            else { w = 4 + ((tid - 127) >> 5); b = (tid - 127) & 31; }
+            d = (dirty[cur][w] >> b) & 1u;
+        }
+        const unsigned bal = __ballot_sync(0xFFFFFFFFu, d);
+        if (lane == 0) wcount[warp] = __popc(bal);
+        __syncthreads();
+        int off = 0, total = 0;
+        #pragma unroll
+        for (int w = 0; w < NT / 32; ++w) {
+            off += w < warp ? wcount[w] : 0;
+            total += wcount[w];
+        }
+        if (d) list[off + __popc(bal & ((1u << lane) - 1u))] = uint16_t(tid);
+        if (total == 0) return it;
+        __syncthreads();
+        uint32_t mark[6] = {0, 0, 0, 0, 0, 0};
+        bool changed = false;
+        if (tid < total) changed = walk_id<NL>(S, dS, wS, vS, vokS, list[tid], mark);
+        if (warp * 32 < total) {   // warps that walked: OR their marks into the next set
+            #pragma unroll
+            for (int w = 0; w < 6; ++w) {
+                const uint32_t m = __reduce_or_sync(0xFFFFFFFFu, mark[w]);
+                if (lane == 0 && m) atomicOr(&dirty[cur ^ 1][w], m);
+            }
+            if (__any_sync(0xFFFFFFFFu, changed) && lane == 0) sh.any = 1;
+        }
+        cur ^= 1;
+        if (it + 1 >= MAX_IT) {
+            __syncthreads();
+            bool left = false;
+            if (tid < 6) left = dirty[cur][tid] != 0;
+            if (__syncthreads_or(left)) requeue = true;
+            return it + 1;
+        }
     }
 }
 
@@ -429,15 +559,29 @@ __device__ void visit_tile(const SolveArgs& a, int s, int tile, int round, unsig
     uint32_t* tgS = vokS + WLS;
     __shared__ VisitShared sh;
     const DT INF = Lim<DT>::INF;
-    if (tid == 0) { sh.marks = 0; sh.any = 0; sh.wide = 0; sh.iters = 0; sh.tmin = ~0ull; sh.wmax = 0; }
+    if (tid == 0) {
+        sh.marks = 0; sh.any = 0; sh.wide = 0; sh.iters = 0; sh.tmin = ~0ull; sh.wmax = 0;
+        // which halo sides changed since the last visit; taken before the halo is read, so a neighbour that
+        // marks us afterwards has also queued us for the next round with the bit still set
+        sh.sides = atomicExch(S.sides + tile, 0u);
+        __threadfence();   // the halo reads below come after the exchange that saw the neighbours' marks
+    }
+    __syncthreads();
 
     // ---- stage
     stage_dist<DT>(S, dS, x0, y0);
     unsigned long long wmax = 0;
     bool wide = false;
+    bool fallback = false;   // joint search whose weights do not fit 16 bits in this tile: general relaxation
     if (joint) {
-        // integer weights of the x, y and diagonal move classes of every state
-        uint32_t* wS = reinterpret_cast<uint32_t*>(smem + L.w);
+        // integer weights of the x, y and diagonal move classes of every state, 16 bits each (0xFFFF impassable)
+        uint16_t* wS = reinterpret_cast<uint16_t*>(smem + L.w);
+        bool big = false;
+        auto w16 = [&](uint32_t w) -> uint16_t {
+            if (w >= INF32) return 0xFFFFu;
+            if (w >= 0xFFFFu) { big = true; return 0xFFFEu; }
+            return uint16_t(w);
+        };
         for (int idx = tid; idx < nl * TILE * TILE; idx += NT) {
             const int l = idx >> 10, r = (idx >> 5) & 31, c = idx & 31;
             const float cf = S.cf[(size_t(l) * hpad + y0 + r) * pitch + x0 + c];
@@ -445,12 +589,20 @@ __device__ void visit_tile(const SolveArgs& a, int s, int tile, int round, unsig
             const uint32_t wx = qweight<uint32_t>(cf, S.fac[l][0]), wy = qweight<uint32_t>(cf, S.fac[l][2]);
             const uint32_t wd = qweight<uint32_t>(cf, S.fac[l][4]);
             const int o = l * WLS + r * CSTR + c;
-            wS[o] = wx;
-            if (S.K == 3) wS[nl * WLS + o] = wy;
-            wS[(S.K - 1) * nl * WLS + o] = wd;
+            wS[o] = w16(wx);
+            if (S.K == 3) wS[nl * WLS + o] = w16(wy);
+            wS[(S.K - 1) * nl * WLS + o] = w16(wd);
             if (cf < 1e30f) {
                 const uint32_t mw = max(max(wx < INF32 ? wx : 0u, wy < INF32 ? wy : 0u), wd < INF32 ? wd : 0u);
                 wmax = max(wmax, static_cast<unsigned long long>(mw));
+            }
+        }
+        fallback = __syncthreads_or(big);
+        if (fallback) {  // the same region now holds the float cost factors of the general relaxation
+            float* cS = reinterpret_cast<float*>(smem + L.w);
+            for (int idx = tid; idx < nl * TILE * TILE; idx += NT) {
+                const int l = idx >> 10, r = (idx >> 5) & 31, c = idx & 31;
+                cS[l * WLS + r * CSTR + c] = S.cf[(size_t(l) * hpad + y0 + r) * pitch + x0 + c];
             }
         }
     } else {
@@ -476,8 +628,8 @@ __device__ void visit_tile(const SolveArgs& a, int s, int tile, int round, unsig
     // ---- relax to a local fixed point
     bool requeue = false;
     int iters;
-    if (joint) {
-        const uint32_t* wS = reinterpret_cast<const uint32_t*>(smem + L.w);
+    if (joint && !fallback) {
+        const uint16_t* wS = reinterpret_cast<const uint16_t*>(smem + L.w);
         uint32_t* d32 = reinterpret_cast<uint32_t*>(dS);
         const uint32_t* v32 = reinterpret_cast<const uint32_t*>(vS);
         switch (nl) {
@@ -543,6 +695,7 @@ __device__ void visit_tile(const SolveArgs& a, int s, int tile, int round, unsig
             }
         }
         if (marks) atomicOr(&sh.marks, marks);
+        __threadfence();   // the written distances are visible device-wide before any neighbour is marked
     }
     if (tid == 0) sh.iters = unsigned(iters);
     __syncthreads();
@@ -557,9 +710,13 @@ __device__ void visit_tile(const SolveArgs& a, int s, int tile, int round, unsig
             if (!((m >> b) & 1)) continue;
             const int nx = tx + DXs[b], ny = ty + DYs[b];
             if (nx < 0 || ny < 0 || nx >= S.ntx || ny >= S.nty) continue;
+            atomicOr(S.sides + ny * S.ntx + nx, opposite_side(b));   // the side of the neighbour facing us
             enqueue(a, S, s, ny * S.ntx + nx, round + 1);
         }
-        if (requeue) enqueue(a, S, s, tile, round + 1);
+        if (requeue) {
+            atomicOr(S.sides + tile, SIDE_ALL);
+            enqueue(a, S, s, tile, round + 1);
+        }
         atomicAdd(a.visits, 1ull);
         atomicAdd(a.visits + 1, static_cast<unsigned long long>(nl));
         atomicAdd(a.visits + 2, static_cast<unsigned long long>(sh.iters));
@@ -581,7 +738,7 @@ __global__ void __launch_bounds__(NT) relax_kernel(SolveArgs a) {
             if (threadIdx.x == 0) {
                 const unsigned int k = atomicAdd(a.ctl + C_NEXT + buf, 1u);
                 if (k < cnt) {
-                    const unsigned long long it = a.wl[size_t(buf) * a.cap + k];
+                    const unsigned long long it = __ldcg(a.wl + size_t(buf) * a.cap + k);   // written last round
                     sh_item_hi = unsigned(it >> 32);
                     sh_item_lo = unsigned(it & 0xFFFFFFFFu);
                 } else {
@@ -636,7 +793,10 @@ __global__ void seed_kernel(SolveArgs a, const uint32_t* const* sidx, const uint
         for (int dy = -1; dy <= 1; ++dy)
             for (int dx = -1; dx <= 1; ++dx) {
                 const int nx = tx + dx, ny = ty + dy;
-                if (nx >= 0 && ny >= 0 && nx < S.ntx && ny < S.nty) enqueue(a, S, s, ny * S.ntx + nx, 1);
+                if (nx >= 0 && ny >= 0 && nx < S.ntx && ny < S.nty) {
+                    atomicOr(S.sides + ny * S.ntx + nx, SIDE_ALL);
+                    enqueue(a, S, s, ny * S.ntx + nx, 1);
+                }
             }
     }
 }
@@ -757,11 +917,11 @@ int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream
         nlmax = std::max(nlmax, b.nl);
     }
     size_t smem = 0;
-    if (kmax) smem = std::max(smem, layout(nlmax, kmax, 4).total);
-    if (any_general) smem = std::max(smem, layout(nlmax, 1, sizeof(DT)).total);
+    if (kmax) smem = std::max(smem, layout(nlmax, joint_wbytes(kmax), 4).total);
+    if (any_general) smem = std::max(smem, layout(nlmax, 4, sizeof(DT)).total);
     Arena& A = g_arena;
     const unsigned int cap = unsigned(std::max<size_t>(tiles, 1));
-    if (!A.dist.need(dbytes) || !A.stamp.need(tiles * 4 + 4) || !A.wl.need(size_t(3) * cap * 8) ||
+    if (!A.dist.need(dbytes) || !A.stamp.need(tiles * 8 + 8) || !A.wl.need(size_t(3) * cap * 8) ||
         !A.sdev.need(sizeof(SDev) * m) || !A.sstat.need(sizeof(SStat) * m) || !A.ctl.need(C_N * 4) ||
         !A.visits.need(24) || !A.sptr.need(size_t(m) * (8 + 8 + 4) + 64)) {
         t_err = "device allocation failed";
@@ -770,6 +930,7 @@ int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream
     for (int k = 0; k < m; ++k) {
         sd[k].dist = static_cast<unsigned char*>(A.dist.p) + doff[k];
         sd[k].stamp = static_cast<uint32_t*>(A.stamp.p) + toff[k];
+        sd[k].sides = static_cast<uint32_t*>(A.stamp.p) + tiles + toff[k];
     }
     std::vector<const uint32_t*> sip(m);
     std::vector<const uint64_t*> sdp(m);
@@ -787,7 +948,7 @@ int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream
     cudaMemcpyAsync(sp + size_t(m) * 8, sdp.data(), size_t(m) * 8, cudaMemcpyHostToDevice, stream);
     cudaMemcpyAsync(sp + size_t(m) * 16, nsv.data(), size_t(m) * 4, cudaMemcpyHostToDevice, stream);
     cudaMemsetAsync(A.dist.p, 0x7F, dbytes, stream);
-    cudaMemsetAsync(A.stamp.p, 0, tiles * 4 + 4, stream);
+    cudaMemsetAsync(A.stamp.p, 0, tiles * 8 + 8, stream);
     cudaMemsetAsync(A.ctl.p, 0, C_N * 4, stream);
     cudaMemsetAsync(A.visits.p, 0, 24, stream);
     SolveArgs a;
@@ -923,7 +1084,7 @@ extern "C" int64_t pcbg_last_batch_local_iters(void) { return pcbg::last_stats()
 
 static __device__ __align__(256) unsigned char pcbg_noalloc_scratch[
     PCBG_NOALLOC_MAX_STATES * 8 +                                          // distances, room for 64-bit
-    (PCBG_NOALLOC_MAX_STATES / (pcbg::TILE * pcbg::TILE)) * (4 + 3 * 8) +  // tile stamps, 3 worklists
+    (PCBG_NOALLOC_MAX_STATES / (pcbg::TILE * pcbg::TILE)) * (8 + 3 * 8) +  // tile stamps + sides, 3 worklists
     4096];                                                                  // descriptors, control words
 
 namespace pcbg {
@@ -931,7 +1092,7 @@ namespace {
 
 constexpr size_t NA_TILES = PCBG_NOALLOC_MAX_STATES / (TILE * TILE);
 constexpr size_t NA_DIST = size_t(PCBG_NOALLOC_MAX_STATES) * 8;
-constexpr size_t NA_STAMP = NA_TILES * 4;
+constexpr size_t NA_STAMP = NA_TILES * 8;   // stamps, then sides
 constexpr size_t NA_WL = NA_TILES * 3 * 8;
 // offsets in the small area after the worklists
 constexpr size_t NA_SDEV = 0, NA_SSTAT = 1024, NA_CTL = 1088, NA_VIS = 1152, NA_SPTR = 1184;
@@ -978,6 +1139,7 @@ int na_run(pcbg_search* q, unsigned char* base, cudaStream_t stream) {
     unsigned char* small = base + NA_DIST + NA_STAMP + NA_WL;
     S.dist = base;
     S.stamp = reinterpret_cast<uint32_t*>(base + NA_DIST);
+    S.sides = S.stamp + NA_TILES;
     SStat st0;
     st0.ub = ~0ull; st0.maxw = 0; st0.best = ~0ull; st0.maxd = 0; st0.need_wide = 0; st0.pad = 0;
     const void* sptr[2] = {q->start_idx, q->start_d};
@@ -989,6 +1151,7 @@ int na_run(pcbg_search* q, unsigned char* base, cudaStream_t stream) {
     // the array keeps the previous call's contents: clear what must start unreached / zero
     cudaMemsetAsync(base, 0x7F, states * sizeof(DT), stream);
     cudaMemsetAsync(base + NA_DIST, 0, tiles * 4, stream);
+    cudaMemsetAsync(base + NA_DIST + NA_TILES * 4, 0, tiles * 4, stream);
     cudaMemsetAsync(small + NA_CTL, 0, C_N * 4, stream);
     cudaMemsetAsync(small + NA_VIS, 0, 24, stream);
     SolveArgs a;
@@ -1005,7 +1168,7 @@ int na_run(pcbg_search* q, unsigned char* base, cudaStream_t stream) {
     seed_kernel<DT><<<1, 128, 0, stream>>>(a, reinterpret_cast<const uint32_t* const*>(small + NA_SPTR),
                                           reinterpret_cast<const uint64_t* const*>(small + NA_SPTR + 8),
                                           reinterpret_cast<const int*>(small + NA_SPTR + 16));
-    const size_t smem = S.mode ? layout(q->nl, S.K, 4).total : layout(q->nl, 1, sizeof(DT)).total;
+    const size_t smem = S.mode ? layout(q->nl, joint_wbytes(S.K), 4).total : layout(q->nl, 4, sizeof(DT)).total;
     const int blocks = occupancy_blocks<DT>(smem);
     if (blocks <= 0) { na_error("relax kernel cannot be resident%s"); return -1; }
     void* args[] = {&a};

@@ -155,6 +155,13 @@ def test_query_free_direction_factors(gpu, seed):
     _cmp_query(synth.random_query(500 + seed, nx=110, ny=90, nl=2 + seed, free_dirf=True))
 
 
+@pytest.mark.parametrize("seed", range(3))
+def test_query_large_costs(gpu, seed):
+    """Cost factors up to 3e5 (16 x weights far above 65535 but inside 32-bit arithmetic): tiles holding them are
+    relaxed by the general path, the others by the 16-bit joint path, in the same solve."""
+    _cmp_query(synth.random_query(700 + seed, nx=130, ny=100, nl=3, big_costs=True))
+
+
 @pytest.mark.parametrize("corner", [(31, 31), (32, 32), (31, 32), (0, 31), (63, 0), (32, 5), (5, 63)])
 def test_start_on_tile_edges(gpu, corner):
     """Starts on tile edges and corners: the tiles around a start must all relax from it."""
