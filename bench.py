@@ -40,6 +40,10 @@ WORKLOAD = ("batched-search microbenchmark: 4096 seeded single-source single-tar
             "8-32; one step = one wave of 512 searches in one persistent launch")
 BYTES_PER_LAYER_VISIT = 32 * 32 * 13     # per staged layer of a tile: cf 4 + flags 1 + distance read 4 + write 4
 BYTES_PER_TILE_VISIT = 32 * 32 * 4       # per tile: via cost of each cell
+# DRAM bytes moved per algorithmic byte by relax_kernel, from one ncu capture of the 64-search case
+# (dram__bytes_read.sum + dram__bytes_write.sum = 12.83 GB against 13.46 GB algorithmic). A full wave is too large to
+# capture; its traffic grows with the tile visits, so the bench scales this ratio by the launch's algorithmic bytes.
+NCU_TRAFFIC_PER_ALG_BYTE = 0.953
 
 
 def peaks():
@@ -400,7 +404,9 @@ def main():
                        "state_visits_per_state": round(lv * 1024 / max(1, st_done), 3),
                        "local_iters_per_visit": round(iters[0] / max(1, tv), 3)},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": None,
+                         "frac": round(achieved / peak, 4),
+                         "traffic": round(NCU_TRAFFIC_PER_ALG_BYTE * alg_bytes / args.steps / 1e9, 2),
+                         "traffic_unit": "GB per launch (ncu ratio of the 64-search case x algorithmic bytes)",
                          "kernel": "relax_kernel (persistent tile relaxation)",
                          "kernel_ms_per_step": round(kms / args.steps, 3), "peak_kind": peak_kind},
             "gpu_launches": int(launches),
