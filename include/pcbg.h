@@ -155,6 +155,15 @@ float pcbg_last_batch_kernel_ms(void);
 int32_t pcbg_last_batch_launches(void);
 int64_t pcbg_last_batch_local_iters(void);   /* sum over tile visits of local relaxation iterations */
 
+/* ---- the round batcher (no reference counterpart) -----------------------------------------------------------
+ * pcbg_solve / gpu_solve calls that run concurrently, from the router's worker threads (src/router.cpp:2187-2235
+ * runs T of them ahead of the commit point), are solved together: each prepares its inputs on its own slot
+ * stream, then the searches queued at that moment run in one persistent relaxation launch. The leader waits for
+ * searches still preparing at most `us` microseconds (default 2000; 0: never waits). Results never depend on the
+ * grouping. pcbg_batcher_stats reports the launches made and the searches they solved since the library loaded. */
+void pcbg_batch_window(int32_t us);
+void pcbg_batcher_stats(int64_t* batches, int64_t* searches);
+
 /* ---- device-resident congestion cost maps (src/router.cpp:197-211, 383-420, 1880-1999) ---------------------- */
 
 /* The cost maps the searches read, kept in HBM and updated in place: per class k, the static owner grids st[l] / vst

@@ -15,7 +15,7 @@ LIB_PATH = _build.LIB
 # the symbols include/pcbg.h declares (C linkage) and include/gpu.h declares (C++ linkage, mangled)
 PCBG_SYMBOLS = [
     "pcbg_available", "pcbg_configure", "pcbg_solve", "pcbg_host_acquire", "pcbg_host_release", "pcbg_last_error",
-    "pcbg_solve_batch", "pcbg_solve_noalloc", "pcbg_last_batch_tile_visits", "pcbg_last_batch_layer_visits", "pcbg_last_batch_rounds",
+    "pcbg_solve_batch", "pcbg_solve_noalloc", "pcbg_batch_window", "pcbg_batcher_stats", "pcbg_last_batch_tile_visits", "pcbg_last_batch_layer_visits", "pcbg_last_batch_rounds",
     "pcbg_last_batch_kernel_ms", "pcbg_last_batch_launches", "pcbg_last_batch_local_iters", "pcbg_synth_search",
     "pcbg_synth_search_host", "pcbg_costs_create", "pcbg_costs_destroy", "pcbg_costs_set_static",
     "pcbg_costs_set_occupancy", "pcbg_costs_set_history", "pcbg_costs_set_ground", "pcbg_costs_rebuild",
@@ -111,6 +111,10 @@ def load() -> C.CDLL:
     lib.pcbg_last_batch_kernel_ms.restype = C.c_float
     lib.pcbg_last_batch_launches.restype = C.c_int32
     lib.pcbg_last_batch_local_iters.restype = C.c_int64
+    lib.pcbg_batch_window.argtypes = [C.c_int32]
+    lib.pcbg_batch_window.restype = None
+    lib.pcbg_batcher_stats.argtypes = [C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    lib.pcbg_batcher_stats.restype = None
     lib.pcbg_synth_search_host.argtypes = [C.c_uint64, C.c_int32, C.c_int32, C.c_int32, C.c_float, C.c_void_p,
                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]
     lib.pcbg_synth_search_host.restype = C.c_int

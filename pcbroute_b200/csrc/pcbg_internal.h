@@ -86,6 +86,22 @@ struct BatchStats {
 };
 BatchStats& last_stats();
 
+// The round batcher (batcher.cpp): concurrent searches solved in one relaxation launch. A search calls
+// batcher_enter() before it prepares its inputs, then either batcher_submit() (blocks until its batch is solved) or,
+// on an error before submitting, batcher_leave().
+struct BatchResult {
+    int rc = 0;                 // solve_batch's return for the batch
+    std::string error;          // its error text when rc != 0
+    long long tile_visits = 0;  // of the whole batch
+    int batch_size = 0;         // searches solved in the same launch
+    float kernel_ms = 0.f;      // relaxation launch time of the batch
+};
+void batcher_enter();
+void batcher_leave();
+int batcher_submit(BatchItem& item, BatchResult& res);
+void batcher_window(int us);
+void batcher_stats(long long* batches, long long* searches);
+
 inline size_t round_up(size_t x, size_t m) { return (x + m - 1) / m * m; }
 
 }  // namespace pcbg

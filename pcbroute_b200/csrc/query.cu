@@ -11,6 +11,10 @@
 #include <climits>
 #include <cmath>
 #include <cstring>
+#include <chrono>
+#include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
 #include <mutex>
 #include <vector>
 
@@ -99,9 +103,12 @@ template <class T> struct DBuf {
     }
 };
 
-struct Engine {
-    std::mutex mu;                 // one query pipeline at a time (the relaxation launch owns the whole GPU)
+// One slot: a stream and the device buffers of one search's inputs. As in the reference (src/gpu.cu:37-58), a
+// worker thread holds a slot for the whole search, and `slots` searches prepare their inputs concurrently; their
+// relaxations then run together through the round batcher (batcher.cpp).
+struct Slot {
     cudaStream_t stream = nullptr;
+    bool busy = false;
     DBuf<float> cf, vcf, out, lval;
     DBuf<uint16_t> st, vst;
     DBuf<uint8_t> fl, prior;
@@ -111,12 +118,14 @@ struct Engine {
     DBuf<uint32_t> lidx, sidx;
 };
 
-Engine g_eng;
 std::mutex g_cfg_mu;
 int g_slots = 4;
 size_t g_maxn = size_t(48) << 20;
 int g_ok = -1;
 std::once_flag g_once;
+std::vector<Slot*> g_slot_v;            // made on first use; never freed (the library lives as long as the process)
+std::mutex g_slot_mu;
+std::condition_variable g_slot_cv;
 
 std::mutex g_pool_mu;
 std::vector<std::pair<float*, size_t>> g_pool;
@@ -136,12 +145,27 @@ uint64_t start_fixed(float g0) {
         if (e_ != cudaSuccess) { set_error(std::string(#x) + ": " + cudaGetErrorString(e_)); return -1; } \
     } while (0)
 
+double now_s() { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); }
+
+// Where one search's time went (printed per search when PCBG_TIMES is set, like the reference's GPU_TIMES).
+struct SearchTimes {
+    double prep = 0, batch = 0, out = 0, kernel_ms = 0;
+    int batch_size = 0;
+};
+
 // Solve one rectangle. Fills best (window state or -1), ub (float cost of best, 1e30 if none), and out->d.
-int solve_rect(const pcbg_query& q, int rx0, int ry0, int rw, int rh, pcbg_result* out, int64_t& best, float& ub) {
-    Engine& E = g_eng;
+int solve_rect(Slot& E, const pcbg_query& q, int rx0, int ry0, int rw, int rh, pcbg_result* out, int64_t& best, float& ub,
+               SearchTimes& tm) {
+    const double t0 = now_s();
     const int nl = q.nl;
     const size_t RN = size_t(rw) * rh, N = RN * nl;
     if (N > g_maxn) { set_error("window over the state cap"); return -1; }
+    // until it joins the batcher's queue, this search counts as one the batch leader waits for
+    batcher_enter();
+    struct Preparing {
+        bool on = true;
+        ~Preparing() { if (on) batcher_leave(); }
+    } preparing;
     const int pitch = int(round_up(rw, TILE)), hpad = int(round_up(rh, TILE));
     const size_t plane = size_t(pitch) * hpad, PN = plane * nl;
     const bool vias = q.via_cost >= 0;
@@ -230,7 +254,12 @@ int solve_rect(const pcbg_query& q, int rx0, int ry0, int rw, int rh, pcbg_resul
     b.cf = E.cf.p; b.fl = E.fl.p; b.vcf = vias ? E.vcf.p : nullptr;
     b.start_idx = E.sidx.p; b.start_d = E.sd.p; b.n_starts = int(si.size());
     b.out = E.out.p;
-    if (solve_batch(&b, 1, S) != 0) return -1;
+    CK(cudaStreamSynchronize(S));   // the inputs are on the device before the batch launch reads them
+    BatchResult br;
+    preparing.on = false;
+    const double t1 = now_s();
+    if (batcher_submit(b, br) != 0) { set_error(br.error); return -1; }
+    const double t2 = now_s();
     // the field, into a pinned buffer from the pool
     float* d = out->d;
     size_t cap = out->cap;
@@ -243,6 +272,12 @@ int solve_rect(const pcbg_query& q, int rx0, int ry0, int rw, int rh, pcbg_resul
     }
     CK(cudaMemcpyAsync(d, E.out.p, N * 4, cudaMemcpyDeviceToHost, S));
     CK(cudaStreamSynchronize(S));
+    const double t3 = now_s();
+    tm.prep += t1 - t0;
+    tm.batch += t2 - t1;
+    tm.out += t3 - t2;
+    tm.kernel_ms += br.kernel_ms;
+    tm.batch_size = std::max(tm.batch_size, br.batch_size);
     best = -1;
     ub = FINF;
     if (b.best >= 0) {
@@ -254,7 +289,7 @@ int solve_rect(const pcbg_query& q, int rx0, int ry0, int rw, int rh, pcbg_resul
     out->best = best;
     out->rounds = b.rounds;
     out->wide = b.status == 1;
-    out->tile_visits = last_stats().tile_visits;
+    out->tile_visits = br.tile_visits;
     out->ub = ub;
     return 0;
 }
@@ -264,7 +299,6 @@ bool probe_device() {
     if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) return false;
     cudaFuncAttributes fa;
     if (cudaFuncGetAttributes(&fa, resolve_kernel) != cudaSuccess) return false;  // no sm_100a image for this device
-    if (cudaStreamCreateWithFlags(&g_eng.stream, cudaStreamNonBlocking) != cudaSuccess) return false;
     return true;
 }
 
@@ -317,10 +351,41 @@ extern "C" int pcbg_solve(const pcbg_query* qp, pcbg_result* out, int wait) {
     if (!pcbg_available()) { set_error("no usable device"); return PCBG_ERR_FAIL; }
     const pcbg_query& q = *qp;
     if (q.nl < 1 || q.nl > MAX_LAYERS || q.ww < 1 || q.wh < 1) { set_error("bad query"); return PCBG_ERR_FAIL; }
-    Engine& E = g_eng;
-    std::unique_lock<std::mutex> lk(E.mu, std::defer_lock);
-    if (wait) lk.lock();
-    else if (!lk.try_lock()) return PCBG_ERR_BUSY;
+    Slot* sp = nullptr;
+    {
+        std::unique_lock<std::mutex> lk(g_slot_mu);
+        if (g_slot_v.empty()) {
+            std::lock_guard<std::mutex> g(g_cfg_mu);
+            for (int k = 0; k < g_slots; ++k) g_slot_v.push_back(new Slot());
+        }
+        auto free_slot = [&]() -> Slot* {
+            for (Slot* c : g_slot_v)
+                if (!c->busy) return c;
+            return nullptr;
+        };
+        sp = free_slot();
+        if (!sp && !wait) return PCBG_ERR_BUSY;
+        while (!sp) {
+            g_slot_cv.wait(lk);
+            sp = free_slot();
+        }
+        sp->busy = true;
+    }
+    struct Release {
+        Slot* s;
+        ~Release() {
+            {
+                std::lock_guard<std::mutex> g(g_slot_mu);
+                s->busy = false;
+            }
+            g_slot_cv.notify_one();
+        }
+    } release{sp};
+    Slot& E = *sp;
+    if (!E.stream && cudaStreamCreateWithFlags(&E.stream, cudaStreamNonBlocking) != cudaSuccess) {
+        set_error("stream creation failed");
+        return PCBG_ERR_FAIL;
+    }
     set_error("");
     const size_t FWN = size_t(q.ww) * q.wh, WS = FWN * q.nl, WB = WS / 64 + 1;
     cudaStream_t S = E.stream;
@@ -366,6 +431,8 @@ extern "C" int pcbg_solve(const pcbg_query* qp, pcbg_result* out, int wait) {
     auto lb = [&](int i, int j) { return oct(i, j, sx0, sy0, sx1, sy1) + oct(i, j, tx0, ty0, tx1, ty1); };
     const int hx0 = std::min(sx0, tx0), hy0 = std::min(sy0, ty0), hx1 = std::max(sx1, tx1), hy1 = std::max(sy1, ty1);
     int M = 80, tries = 0;
+    SearchTimes tm;
+    const double t_start = now_s();
     out->best = -1;
     for (;; M *= 3, ++tries) {
         int rx0 = std::max(0, hx0 - M), ry0 = std::max(0, hy0 - M);
@@ -374,7 +441,7 @@ extern "C" int pcbg_solve(const pcbg_query* qp, pcbg_result* out, int wait) {
         const bool full = rx0 == 0 && ry0 == 0 && rx1 == q.ww && ry1 == q.wh;
         int64_t best = -1;
         float ub = FINF;
-        if (solve_rect(q, rx0, ry0, rx1 - rx0, ry1 - ry0, out, best, ub) != 0) return PCBG_ERR_FAIL;
+        if (solve_rect(E, q, rx0, ry0, rx1 - rx0, ry1 - ry0, out, best, ub, tm) != 0) return PCBG_ERR_FAIL;
         if (full) break;
         if (ub < FINF * 0.5f) {
             const double lim = double(ub) * 1.0001 + 1e-3;
@@ -387,5 +454,12 @@ extern "C" int pcbg_solve(const pcbg_query* qp, pcbg_result* out, int wait) {
         }
     }
     out->tries = tries + 1;
+    static const bool report = std::getenv("PCBG_TIMES") != nullptr;
+    if (report)
+        std::fprintf(stderr,
+                     "pcbg: window %dx%dx%d rect %dx%d (%d tries) prep %.2f ms, batch %.2f ms (%d searches, relax %.2f ms), "
+                     "field %.2f ms, total %.2f ms\n",
+                     q.ww, q.wh, q.nl, out->rw, out->rh, tries + 1, tm.prep * 1e3, tm.batch * 1e3, tm.batch_size,
+                     tm.kernel_ms, tm.out * 1e3, (now_s() - t_start) * 1e3);
     return std::max(1, out->rounds);
 }

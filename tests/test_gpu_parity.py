@@ -274,3 +274,44 @@ def test_wide_distances(gpu):
     q.tbit[t >> 6] |= np.uint64(1) << np.uint64(t & 63)
     out, ref = _cmp_query(q)
     assert out.wide and out.best == t and ref.ub > 5e6
+
+
+def test_concurrent_queries_are_batched_and_exact(gpu):
+    """Queries from 8 threads at once (the router's worker threads) run through the round batcher: the launches
+    solve several searches each, and every result is the oracle's, whatever the grouping."""
+    import threading
+    lib = _lib.load()
+    qs = [synth.random_query(700 + k, nx=150, ny=110, nl=2 + k % 5, prior=k % 3 == 0) for k in range(24)]
+    refs = [oracle.solve(q) for q in qs]
+    b0, s0 = C.c_int64(), C.c_int64()
+    lib.pcbg_batcher_stats(C.byref(b0), C.byref(s0))
+    outs = [None] * len(qs)
+    errs = []
+
+    def work(w):
+        try:
+            for k in range(w, len(qs), 8):
+                out = query.GpuOut()
+                outs[k] = (query.gpu_solve(qs[k], out), out)
+        except Exception as e:  # surfaced below
+            errs.append(e)
+
+    ts = [threading.Thread(target=work, args=(w,)) for w in range(8)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    assert not errs, errs
+    b1, s1 = C.c_int64(), C.c_int64()
+    lib.pcbg_batcher_stats(C.byref(b1), C.byref(s1))
+    searches, batches = s1.value - s0.value, b1.value - b0.value
+    assert searches >= len(qs)
+    assert batches < searches, (batches, searches)    # some launches solved more than one search
+    for (rc, out), (orc, ref) in zip(outs, refs):
+        if orc < 0:
+            assert rc == -1
+            continue
+        assert rc >= 1
+        assert (out.rx0, out.ry0, out.rw, out.rh, out.best, out.tries) == \
+            (ref.rx0, ref.ry0, ref.rw, ref.rh, ref.best, ref.tries)
+        assert np.array_equal(out.d.view(np.uint32), ref.d.view(np.uint32))
