@@ -110,6 +110,9 @@ typedef struct pcbg_search {
     const uint64_t* start_d;    /* device fixed-point start costs */
     int32_t n_starts;
     float* out;                 /* device [nl][rh][rw] reported field, or NULL */
+    uint32_t* path;             /* device, or NULL: the walk-back from best to a start (rect states, best first) */
+    int32_t path_cap;           /* capacity of path, in states */
+    int32_t* path_len;          /* device: states written; 0 if no target was reached, -1 if no walk fits path_cap */
     /* results */
     int64_t best;               /* rect state of the cheapest target, -1 if none */
     uint64_t best_d;            /* its fixed-point cost */
@@ -194,10 +197,57 @@ const float* pcbg_costs_device_map(pcbg_costs* h, int32_t cls, int32_t layer);
 /* Mean device time (ms, CUDA events) of `reps` full rebuilds. */
 float pcbg_costs_time_rebuild(pcbg_costs* h, float pres, int32_t hard, int32_t reps);
 
+/* ---- speculative negotiation rounds on the device (src/router.cpp:2096-2242, route_waves) ----------------------
+ * A fixed order of nets is routed against a cost board (pcbg_costs, one class). The nets a policy picks from the
+ * lookahead window of the commit point are searched together in one persistent launch, walked back on the device,
+ * and committed in order: a net is accepted if no commit since its search started crossed a block (8 x 8 cells)
+ * of its window, else it is searched again (a wasted search). Every policy gives the paths of the sequential one. */
+typedef struct pcbg_net {
+    int32_t x0, y0, x1, y1;     /* search window [x0, x1) x [y0, y1) on the board */
+    uint32_t src, tgt;          /* board states l * nx * ny + y * nx + x, inside the window */
+} pcbg_net;
+
+typedef struct pcbg_spec_stats {
+    int64_t searches;           /* searches run, speculative ones included */
+    int64_t wasted;             /* searches thrown away at commit */
+    int64_t batches;            /* persistent launches */
+    int64_t commits;
+    int64_t conflicts;          /* nets whose path shares a state with another net's path */
+    double search_ms;           /* host time in the batched searches (resolve, launch, walk-back, paths read) */
+    double total_ms;
+} pcbg_spec_stats;
+
+typedef struct pcbg_spec pcbg_spec;
+
+#define PCBG_SPEC_SEQUENTIAL 0  /* one net per launch: the order's own result */
+#define PCBG_SPEC_PLAIN 1       /* every open net of the lookahead window (route_waves' workers) */
+#define PCBG_SPEC_LEARNED 2     /* the nets the attached scheduler picks; PLAIN when none is attached */
+
+/* Learned batch composition: given the commit point and the open candidates of the window (ascending), set
+ * pick[k] != 0 for the candidates to search now (the net at the commit point is always searched). Returns 0. */
+typedef int (*pcbg_spec_scheduler)(void* user, pcbg_spec* s, int32_t cursor, const int32_t* cand, int32_t n,
+                                   int32_t* pick);
+/* Called before each search with the commit point: the nets [cursor, net) are not committed yet. */
+typedef void (*pcbg_spec_observer)(void* user, pcbg_spec* s, int32_t cursor, int32_t net);
+
+pcbg_spec* pcbg_spec_create(pcbg_costs* costs, int32_t cls, const pcbg_net* nets, int32_t n, float via_cost);
+void pcbg_spec_destroy(pcbg_spec* s);
+void pcbg_spec_set_scheduler(pcbg_spec* s, pcbg_spec_scheduler f, void* user);
+void pcbg_spec_set_observer(pcbg_spec* s, pcbg_spec_observer f, void* user);
+/* One rip-up-and-reroute iteration at present-congestion factor pres: lift every path, rebuild the costs, route
+ * all nets in order with the policy (width: the lookahead, adapted as route_waves does). */
+int pcbg_spec_iterate(pcbg_spec* s, float pres, int32_t policy, int32_t width, pcbg_spec_stats* st);
+/* A net's committed path (board states, target first); returns its length. */
+int32_t pcbg_spec_path(pcbg_spec* s, int32_t net, uint32_t* states, int32_t cap);
+/* History += inc on every state two or more paths share (count_conflicts); returns how many. */
+int32_t pcbg_spec_add_history(pcbg_spec* s, float inc);
+/* 1 if a path through these board states would invalidate a search of net's window, else 0. */
+int32_t pcbg_spec_window_reads(pcbg_spec* s, int32_t net, const uint32_t* states, int32_t m);
+
 /* ---- seeded synthetic search generator (the batched-search microbenchmark workload) ----------------------- */
 
 /* Fill a pitched search with the seeded workload: per (layer, cell) cost 1 + (h % 16), about 15 % of cells
- * blocked in value-noise blobs (the same on every layer), via cost `via` per cell, flags, one source and one
+ * blocked in value-noise blobs (drawn per layer), via cost `via` per cell, flags, one source and one
  * target picked among free cells. cf/flags/vcf are the pcbg_search device arrays; src/tgt receive the rect
  * states chosen (device int64 each). Deterministic in (seed). */
 int pcbg_synth_search(uint64_t seed, int32_t rw, int32_t rh, int32_t nl, int32_t pitch, int32_t hpad, float via,

@@ -47,6 +47,9 @@ def lib() -> C.CDLL:
         L.pcbo_dijkstra.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_uint64)]
         L.pcbo_dijkstra.restype = C.c_int64
+        L.pcbo_walkback.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64]
+        L.pcbo_walkback.restype = C.c_int64
         L.pcbo_report.argtypes = [C.c_int64, C.c_void_p, C.c_int64, C.c_uint64, C.c_void_p]
         L.pcbo_resolve.argtypes = [C.POINTER(plib.Query), C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                    C.c_void_p]
@@ -114,6 +117,24 @@ def dijkstra(fac: np.ndarray, cf: np.ndarray, flags: np.ndarray, vcf, start_idx,
                                None if vcf is None else vcf.ctypes.data, len(si), si.ctypes.data, sd.ctypes.data,
                                dist.ctypes.data, C.byref(bd))
     return dist, int(best), int(bd.value)
+
+
+def walkback(fac: np.ndarray, cf: np.ndarray, flags: np.ndarray, vcf, start_idx, start_dv, dist: np.ndarray, best: int,
+             cap: int = 1 << 20) -> np.ndarray | None:
+    """Path (rect states, best first) of pcbo_walkback, [] if best < 0, None if the walk fails."""
+    nl, rh, rw = cf.shape
+    fac = np.ascontiguousarray(fac, np.float32)
+    cf = np.ascontiguousarray(cf, np.float32)
+    flags = np.ascontiguousarray(flags, np.uint8)
+    vcf = None if vcf is None else np.ascontiguousarray(vcf, np.float32)
+    si = np.ascontiguousarray(start_idx, np.uint32)
+    sd = np.ascontiguousarray(start_dv, np.uint64)
+    d = np.ascontiguousarray(dist, np.uint64)
+    path = np.empty(cap, np.uint32)
+    n = lib().pcbo_walkback(rw, rh, nl, fac.ctypes.data, cf.ctypes.data, flags.ctypes.data,
+                            None if vcf is None else vcf.ctypes.data, len(si), si.ctypes.data, sd.ctypes.data,
+                            d.ctypes.data, best, path.ctypes.data, cap)
+    return None if n < 0 else path[:n].copy()
 
 
 def report(dist: np.ndarray, best: int, best_d: int) -> np.ndarray:

@@ -191,6 +191,41 @@ int64_t pcbo_dijkstra(int rw, int rh, int nl, const float fac[8][8], const float
     return best;
 }
 
+int64_t pcbo_walkback(int rw, int rh, int nl, const float fac[8][8], const float* cf, const uint8_t* flags,
+                      const float* vcf, int64_t n_starts, const uint32_t* start_idx, const uint64_t* start_d,
+                      const uint64_t* dist, int64_t best, uint32_t* path, int64_t cap) {
+    if (best < 0) return 0;
+    const size_t RN = (size_t)rw * rh;
+    size_t q = (size_t)best;
+    for (int64_t n = 0; n < cap; ++n) {
+        const int l = (int)(q / RN);
+        const size_t c = q % RN;
+        const int j = (int)(c / rw), i = (int)(c % rw);
+        const uint64_t dq = dist[q];
+        path[n] = (uint32_t)q;
+        for (int64_t k = 0; k < n_starts; ++k)
+            if (start_idx[k] == (uint32_t)q && start_d[k] < PCBO_INF64 && start_d[k] == dq) return n + 1;
+        int found = 0;
+        for (int m = 0; m < 8 && !found; ++m) {           /* p -> q by move m: p = q - (MDX[m], MDY[m]) */
+            const int pi = i - MDX[m], pj = j - MDY[m];
+            if (pi < 0 || pj < 0 || pi >= rw || pj >= rh) continue;
+            const size_t p = (size_t)l * RN + (size_t)pj * rw + pi;
+            const uint64_t w = pcbo_weight(cf[q], fac[l][m]);
+            if (w != PCBO_INF64 && dist[p] != PCBO_INF64 && dist[p] + w == dq) { q = p; found = 1; }
+        }
+        if (!found && vcf && (flags[q] & 1)) {
+            const uint64_t w = pcbo_weight(vcf[c], 1.0f);
+            for (int l2 = 0; l2 < nl && !found && w != PCBO_INF64; ++l2) {
+                if (l2 == l) continue;
+                const size_t p = (size_t)l2 * RN + c;
+                if (dist[p] != PCBO_INF64 && dist[p] + w == dq) { q = p; found = 1; }
+            }
+        }
+        if (!found) return -1;
+    }
+    return -1;
+}
+
 void pcbo_report(int64_t n, const uint64_t* dist, int64_t best, uint64_t best_d, float* out) {
     for (int64_t s = 0; s < n; ++s) {
         const uint64_t d = dist[s];

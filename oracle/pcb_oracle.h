@@ -48,6 +48,14 @@ int64_t pcbo_dijkstra(int rw, int rh, int nl, const float fac[8][8], const float
                       const float* vcf, int64_t n_starts, const uint32_t* start_idx, const uint64_t* start_d,
                       uint64_t* dist, uint64_t* best_d);
 
+/* Walk-back over an exact field from `best` to a start (src/router.cpp:1615-1679 order): at each state stop if it
+ * is a start at its own start cost, else step to the first predecessor, moves 0-7 then via layers ascending, whose
+ * distance plus the move's weight equals this state's. Writes rect states, best first. Returns the states written,
+ * 0 if best < 0, -1 if no predecessor exists or the walk exceeds cap. */
+int64_t pcbo_walkback(int rw, int rh, int nl, const float fac[8][8], const float* cf, const uint8_t* flags,
+                      const float* vcf, int64_t n_starts, const uint32_t* start_idx, const uint64_t* start_d,
+                      const uint64_t* dist, int64_t best, uint32_t* path, int64_t cap);
+
 /* The reported float field of a solved rectangle: d / 16 where d <= d(best) (every reached state if best < 0). */
 void pcbo_report(int64_t n, const uint64_t* dist, int64_t best, uint64_t best_d, float* out);
 

@@ -15,7 +15,9 @@ LIB_PATH = _build.LIB
 # the symbols include/pcbg.h declares (C linkage) and include/gpu.h declares (C++ linkage, mangled)
 PCBG_SYMBOLS = [
     "pcbg_available", "pcbg_configure", "pcbg_solve", "pcbg_host_acquire", "pcbg_host_release", "pcbg_last_error",
-    "pcbg_solve_batch", "pcbg_solve_noalloc", "pcbg_batch_window", "pcbg_batcher_stats", "pcbg_last_batch_tile_visits", "pcbg_last_batch_layer_visits", "pcbg_last_batch_rounds",
+    "pcbg_solve_batch", "pcbg_solve_noalloc", "pcbg_batch_window", "pcbg_batcher_stats", "pcbg_spec_create",
+    "pcbg_spec_destroy", "pcbg_spec_set_scheduler", "pcbg_spec_set_observer", "pcbg_spec_iterate", "pcbg_spec_path",
+    "pcbg_spec_add_history", "pcbg_spec_window_reads", "pcbg_last_batch_tile_visits", "pcbg_last_batch_layer_visits", "pcbg_last_batch_rounds",
     "pcbg_last_batch_kernel_ms", "pcbg_last_batch_launches", "pcbg_last_batch_local_iters", "pcbg_synth_search",
     "pcbg_synth_search_host", "pcbg_costs_create", "pcbg_costs_destroy", "pcbg_costs_set_static",
     "pcbg_costs_set_occupancy", "pcbg_costs_set_history", "pcbg_costs_set_ground", "pcbg_costs_rebuild",
@@ -77,10 +79,27 @@ class Search(C.Structure):
         ("cf", C.c_void_p), ("flags", C.c_void_p), ("vcf", C.c_void_p),
         ("start_idx", C.c_void_p), ("start_d", C.c_void_p), ("n_starts", C.c_int32),
         ("out", C.c_void_p),
+        ("path", C.c_void_p), ("path_cap", C.c_int32), ("path_len", C.c_void_p),
         ("best", C.c_int64), ("best_d", C.c_uint64),
         ("status", C.c_int32), ("rounds", C.c_int32),
     ]
 
+
+class Net(C.Structure):
+    """struct pcbg_net: a net of a speculative round (window and pins as board states)."""
+    _fields_ = [("x0", C.c_int32), ("y0", C.c_int32), ("x1", C.c_int32), ("y1", C.c_int32),
+                ("src", C.c_uint32), ("tgt", C.c_uint32)]
+
+
+class SpecStats(C.Structure):
+    """struct pcbg_spec_stats."""
+    _fields_ = [("searches", C.c_int64), ("wasted", C.c_int64), ("batches", C.c_int64), ("commits", C.c_int64),
+                ("conflicts", C.c_int64), ("search_ms", C.c_double), ("total_ms", C.c_double)]
+
+
+SCHEDULER = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.c_int32,
+                        C.POINTER(C.c_int32))
+OBSERVER = C.CFUNCTYPE(None, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32)
 
 _lib = None
 
@@ -111,6 +130,22 @@ def load() -> C.CDLL:
     lib.pcbg_last_batch_kernel_ms.restype = C.c_float
     lib.pcbg_last_batch_launches.restype = C.c_int32
     lib.pcbg_last_batch_local_iters.restype = C.c_int64
+    lib.pcbg_spec_create.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_float]
+    lib.pcbg_spec_create.restype = C.c_void_p
+    lib.pcbg_spec_destroy.argtypes = [C.c_void_p]
+    lib.pcbg_spec_destroy.restype = None
+    lib.pcbg_spec_set_scheduler.argtypes = [C.c_void_p, SCHEDULER, C.c_void_p]
+    lib.pcbg_spec_set_scheduler.restype = None
+    lib.pcbg_spec_set_observer.argtypes = [C.c_void_p, OBSERVER, C.c_void_p]
+    lib.pcbg_spec_set_observer.restype = None
+    lib.pcbg_spec_iterate.argtypes = [C.c_void_p, C.c_float, C.c_int32, C.c_int32, C.POINTER(SpecStats)]
+    lib.pcbg_spec_iterate.restype = C.c_int
+    lib.pcbg_spec_path.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]
+    lib.pcbg_spec_path.restype = C.c_int32
+    lib.pcbg_spec_add_history.argtypes = [C.c_void_p, C.c_float]
+    lib.pcbg_spec_add_history.restype = C.c_int32
+    lib.pcbg_spec_window_reads.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]
+    lib.pcbg_spec_window_reads.restype = C.c_int32
     lib.pcbg_batch_window.argtypes = [C.c_int32]
     lib.pcbg_batch_window.restype = None
     lib.pcbg_batcher_stats.argtypes = [C.POINTER(C.c_int64), C.POINTER(C.c_int64)]

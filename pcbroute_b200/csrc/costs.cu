@@ -396,6 +396,23 @@ extern "C" int pcbg_costs_download_history(pcbg_costs* h, float* hist) {
     return 0;
 }
 
+bool pcbg::cost_planes(pcbg_costs* h, int cls, CostPlanes& o) {
+    if (!h || cls < 0 || cls >= h->D.nclasses) return false;
+    memset(&o, 0, sizeof(o));
+    o.nx = h->nx;
+    o.ny = h->ny;
+    o.nl = h->D.nl;
+    for (int l = 0; l < h->D.nl; ++l) {
+        const int id = cls * pcbg::MAX_LAYERS + l;
+        o.cst[l] = h->D.cst[id];
+        o.oc[l] = h->D.oc[id];
+        o.ov[l] = h->D.ov[id];
+        o.hist[l] = h->D.hist[l];
+    }
+    o.vcst = h->D.vcst[cls];
+    return true;
+}
+
 extern "C" const float* pcbg_costs_device_map(pcbg_costs* h, int32_t cls, int32_t layer) {
     if (!h || cls < 0 || cls >= h->D.nclasses || layer < -1 || layer >= h->D.nl) return nullptr;
     return layer < 0 ? h->D.vcst[cls] : h->D.cst[cls * pcbg::MAX_LAYERS + layer];

@@ -5,7 +5,9 @@
 #include <cstdint>
 #include <string>
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <vector>
 
 #include "pcbg.h"
 
@@ -39,6 +41,9 @@ struct SDev {
     uint32_t* stamp;
     uint32_t* sides;   // per tile: which halo sides changed since its last visit (bit 8: everything)
     float* out;
+    uint32_t* path;    // walk-back output (or null), capacity path_cap; its length goes to *path_len
+    int* path_len;
+    int path_cap;
 };
 
 // Per-search statistics written by the kernels.
@@ -62,6 +67,9 @@ struct BatchItem {
     const uint64_t* start_d;     // device
     int n_starts;
     float* out;
+    uint32_t* path;              // device, or null: walk-back from best to a start
+    int path_cap;
+    int* path_len;               // device
     // results
     int64_t best;
     uint64_t best_d;
@@ -101,6 +109,44 @@ void batcher_leave();
 int batcher_submit(BatchItem& item, BatchResult& res);
 void batcher_window(int us);
 void batcher_stats(long long* batches, long long* searches);
+
+// Device planes of one class of a cost board (costs.cu), for kernels outside it that read the board in place.
+struct CostPlanes {
+    int nx, ny, nl;
+    const float* cst[MAX_LAYERS];
+    const float* vcst;
+    const uint8_t* oc[MAX_LAYERS];
+    const uint8_t* ov[MAX_LAYERS];
+    const float* hist[MAX_LAYERS];
+};
+bool cost_planes(pcbg_costs* h, int cls, CostPlanes& out);
+
+// The conflict predictor's network (mlp.cu): D0 inputs (two 32 x 32 rasters, an 8 x 8 overlap mask, 64 scalars),
+// two hidden layers of MLP_H, one logit. BF16 operands, FP32 accumulation, FP32 master weights under Adam.
+constexpr int MLP_D0 = 2 * 1024 + 64 + 64, MLP_H = 128;
+struct Mlp {
+    // f32 parameters, packed: W1 [H][D0], W2 [H][H], b1 [H], b2 [H], w3 [H], b3
+    size_t nparams = 0;
+    float *master = nullptr, *grad = nullptr, *m1 = nullptr, *m2 = nullptr;
+    __nv_bfloat16 *w1b = nullptr, *w2b = nullptr, *w2t = nullptr;
+    // activations of the last forward (capacity cap rows)
+    int cap = 0;
+    __nv_bfloat16 *h1 = nullptr, *h1t = nullptr, *h2 = nullptr, *dz2 = nullptr, *dz2t = nullptr, *dz1 = nullptr,
+                  *dz1t = nullptr, *xt = nullptr;
+    float *z3 = nullptr, *lossd = nullptr;
+    int step = 0;
+    std::vector<void*> owned;
+    ~Mlp();
+    bool init(uint64_t seed);
+    int set_params(const float* host);
+    int refresh_bf16(cudaStream_t s);
+    bool reserve(int B);
+    // x [B][D0] bf16 on the device, B a multiple of 64; p (device, may be null): sigmoid of the logits
+    int forward(cudaStream_t s, const __nv_bfloat16* x, int B, float* p);
+    // after forward on the same x: gradients of sum_b w[b] * BCE(z3[b], y[b]) / wsum into grad; loss (host) if set
+    int backward(cudaStream_t s, const __nv_bfloat16* x, const float* y, const float* w, float wsum, int B, float* loss);
+    int adam(cudaStream_t s, float lr);
+};
 
 inline size_t round_up(size_t x, size_t m) { return (x + m - 1) / m * m; }
 

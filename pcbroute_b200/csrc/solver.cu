@@ -833,6 +833,64 @@ __global__ void report_kernel(const SDev* Sv, SStat* stv) {
     }
 }
 
+// Walk-back from the best target to a start over the exact field, one warp per search. At each state q: stop if q
+// is a start at its own start cost; else step to the first predecessor p, in the order moves 0-7 then via layers
+// ascending (the router's walk-back order, src/router.cpp:1615-1679), with d(p) + w(p -> q) == d(q). Every state
+// on the walk has d <= d(best), where the field is exact, so the walk is the oracle's. Lanes 0-7 test the moves,
+// 8-15 the via layers, 16-31 the start list.
+template <typename DT>
+__global__ void walkback_kernel(const SDev* Sv, const SStat* stv, const uint32_t* const* sidx, const uint64_t* const* sd,
+                                const int* ns) {
+    const int s = blockIdx.x, lane = threadIdx.x;
+    const SDev& S = Sv[s];
+    if (!S.path) return;
+    const SStat& st = stv[s];
+    const DT INF = Lim<DT>::INF;
+    if (st.best == ~0ull || st.ub >= static_cast<unsigned long long>(INF)) {
+        if (lane == 0) *S.path_len = 0;
+        return;
+    }
+    const int MX[8] = {1, -1, 0, 0, 1, 1, -1, -1}, MY[8] = {0, 0, 1, -1, 1, -1, 1, -1};
+    const DT* dist = reinterpret_cast<const DT*>(S.dist);
+    const size_t RN = size_t(S.rw) * S.rh;
+    auto at = [&](int l, int j, int i) { return (size_t(l) * S.hpad + j) * S.pitch + i; };
+    unsigned long long q = st.best;
+    int n = 0, result = -1;
+    for (; n < S.path_cap; ++n) {
+        const int l = int(q / RN), rem = int(q % RN), j = rem / S.rw, i = rem % S.rw;
+        const size_t pq = at(l, j, i);
+        const DT dq = dist[pq];
+        if (lane == 0) S.path[n] = uint32_t(q);
+        bool hit = false, start = false;
+        unsigned long long cand = 0;
+        if (lane < 8) {
+            const int pi = i - MX[lane], pj = j - MY[lane];
+            if (pi >= 0 && pj >= 0 && pi < S.rw && pj < S.rh) {
+                const DT w = qweight<DT>(S.cf[pq], S.fac[l][lane]);
+                const DT dp = dist[at(l, pj, pi)];
+                hit = w < INF && dp < INF && dp + w == dq;
+                cand = size_t(l) * RN + size_t(pj) * S.rw + pi;
+            }
+        } else if (lane < 16) {
+            const int l2 = lane - 8;
+            if (S.vcf && l2 < S.nl && l2 != l && (S.fl[pq] & 1)) {
+                const DT w = qweight<DT>(S.vcf[size_t(j) * S.pitch + i], 1.0f);
+                const DT dp = dist[at(l2, j, i)];
+                hit = w < INF && dp < INF && dp + w == dq;
+                cand = size_t(l2) * RN + size_t(j) * S.rw + i;
+            }
+        } else {
+            for (int k = lane - 16; k < ns[s]; k += 16)
+                if (sidx[s][k] == uint32_t(q) && sd[s][k] < uint64_t(INF) && DT(sd[s][k]) == dq) start = true;
+        }
+        if (__any_sync(0xFFFFFFFFu, start)) { result = n + 1; break; }
+        const unsigned b = __ballot_sync(0xFFFFFFFFu, hit);
+        if (!b) break;
+        q = __shfl_sync(0xFFFFFFFFu, cand, __ffs(b) - 1);
+    }
+    if (lane == 0) *S.path_len = result;
+}
+
 // ---- device arena (grow-only; all batch solves are serialised by g_mu) ----
 
 std::mutex g_mu;
@@ -893,7 +951,7 @@ int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream
     std::vector<size_t> doff(m), toff(m);
     size_t dbytes = 0, tiles = 0;
     int nlmax = 1, kmax = 0;
-    bool any_general = false;
+    bool any_general = false, any_path = false;
     for (int k = 0; k < m; ++k) {
         const BatchItem& b = items[idx[k]];
         SDev& S = sd[k];
@@ -910,6 +968,8 @@ int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream
         if (S.mode) kmax = std::max(kmax, S.K);
         else any_general = true;
         S.cf = b.cf; S.fl = b.fl; S.vcf = b.vcf; S.out = b.out;
+        S.path = b.path; S.path_len = b.path_len; S.path_cap = b.path_cap;
+        if (b.path) any_path = true;
         doff[k] = dbytes;
         dbytes += round_up(size_t(b.nl) * b.hpad * b.pitch * sizeof(DT), 256);
         toff[k] = tiles;
@@ -973,6 +1033,10 @@ int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream
     cudaEventRecord(g_ev1, stream);
     report_kernel<DT><<<dim3(32, m), 256, 0, stream>>>(a.S, a.st);
     bs.launches += 3;
+    if (any_path) {
+        walkback_kernel<DT><<<m, 32, 0, stream>>>(a.S, a.st, d_sip, d_sdp, d_ns);
+        bs.launches += 1;
+    }
     std::vector<SStat> st(m);
     unsigned int ctl[C_N];
     unsigned long long visits[3] = {0, 0, 0};
@@ -1057,6 +1121,7 @@ extern "C" int pcbg_solve_batch(pcbg_search* s, int32_t n, void* stream) {
         b.cf = q.cf; b.fl = q.flags; b.vcf = q.vcf;
         b.start_idx = q.start_idx; b.start_d = q.start_d; b.n_starts = q.n_starts;
         b.out = q.out;
+        b.path = q.path; b.path_cap = q.path_cap; b.path_len = q.path_len;
     }
     const int r = pcbg::solve_batch(it.data(), n, static_cast<cudaStream_t>(stream));
     if (r != 0) return PCBG_ERR_FAIL;

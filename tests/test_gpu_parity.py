@@ -54,7 +54,7 @@ def test_device_generator_matches_numpy(gpu, rw, rh, nl):
     assert (full[:, rh:, :] >= 1e30).all() and (full[:, :, rw:] >= 1e30).all()
 
 
-def run_batch(searches, with_out=True):
+def run_batch(searches, with_out=True, with_path=False):
     torch = _torch()
     lib = _lib.load()
     arr = (_lib.Search * len(searches))()
@@ -79,6 +79,13 @@ def run_batch(searches, with_out=True):
             a.out = out.data_ptr()
         else:
             a.out = None
+        if with_path:
+            cap = 4 * (s["rw"] + s["rh"]) * s["nl"] + 64
+            path = torch.empty(cap, dtype=torch.int32, device="cuda")
+            plen = torch.zeros(1, dtype=torch.int32, device="cuda")
+            keep += [path, plen]
+            s["path"], s["plen"] = path, plen
+            a.path, a.path_cap, a.path_len = path.data_ptr(), cap, plen.data_ptr()
     rc = lib.pcbg_solve_batch(arr, len(searches), None)
     assert rc == 0, _lib.last_error()
     torch.cuda.synchronize()
@@ -109,6 +116,32 @@ def test_batch_matches_oracle(gpu):
             assert arr[k].best_d == bd
         got = s["out"].cpu().numpy().reshape(s["nl"], s["rh"], s["rw"])
         assert np.array_equal(got.view(np.uint32), field.view(np.uint32)), k
+
+
+def test_walkback_matches_oracle(gpu):
+    """The device walk-back (one warp per search, after the relaxation) equals the oracle's walk over its exact
+    field: the same states in the same order, best target first, ending on the start."""
+    rng = np.random.default_rng(11)
+    searches = []
+    for k in range(16):
+        rw, rh = int(rng.integers(20, 260)), int(rng.integers(20, 260))
+        searches.append(make_device_search(4200 + k, rw, rh, int(rng.integers(2, 7)), float(rng.integers(8, 33))))
+    arr = run_batch(searches, with_path=True)
+    walked = 0
+    for k, s in enumerate(searches):
+        cf, fl, vcf, src, tgt = synth.search_arrays(s["seed"], s["rw"], s["rh"], s["nl"], s["via"])
+        fac = synth.microbench_factors(s["nl"])
+        si = np.array([src] if src >= 0 else [], np.uint32)
+        sd = np.zeros(len(si), np.uint64)
+        dist, best, bd = oracle.dijkstra(fac, cf, fl, vcf, si, sd)
+        ref = oracle.walkback(fac, cf, fl, vcf, si, sd, dist, best)
+        n = int(s["plen"].item())
+        assert ref is not None
+        assert n == len(ref), (k, n, len(ref))
+        got = s["path"][:n].cpu().numpy().view(np.uint32)
+        assert np.array_equal(got, ref), k
+        walked += n > 0
+    assert walked >= 10
 
 
 def test_batch_without_field_output(gpu):

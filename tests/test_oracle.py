@@ -162,3 +162,35 @@ def test_golden_fixtures():
         assert rc >= 1
         assert np.array_equal(g[name + "_rect"], np.array([out.rx0, out.ry0, out.rw, out.rh, out.best, out.tries])), name
         assert make_golden.digest(out.d) == str(g[name + "_digest"]), name
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_walkback_is_a_shortest_path(seed):
+    """pcbo_walkback: consecutive states are one move or one via apart, each step's weight is exactly the distance
+    difference, the walk starts at the best target and ends at a start at its start cost."""
+    rw, rh, nl = 40 + 7 * seed, 33 + 5 * seed, 2 + seed % 3
+    cf, fl, vcf, src, tgt = synth.search_arrays(300 + seed, rw, rh, nl, 12.0)
+    fac = synth.microbench_factors(nl)
+    si = np.array([src], np.uint32)
+    sd = np.zeros(1, np.uint64)
+    dist, best, bd = O.dijkstra(fac, cf, fl, vcf, si, sd)
+    path = O.walkback(fac, cf, fl, vcf, si, sd, dist, best)
+    if best < 0:
+        assert path is not None and len(path) == 0
+        return
+    assert path is not None and path[0] == best and path[-1] == src
+    d = dist.reshape(-1)
+    RN = rw * rh
+    for q, p in zip(path[:-1], path[1:]):
+        lq, cq = divmod(int(q), RN)
+        lp, cp = divmod(int(p), RN)
+        jq, iq = divmod(cq, rw)
+        jp, ip = divmod(cp, rw)
+        if lq == lp:
+            m = [k for k in range(8) if (iq - ip, jq - jp) == (DX[k], DY[k])]
+            assert len(m) == 1
+            w = O.weight(float(cf.reshape(-1)[q]), float(fac[lq, m[0]]))
+        else:
+            assert cq == cp and fl.reshape(-1)[q] & 1
+            w = O.weight(float(vcf.reshape(-1)[cq]), 1.0)
+        assert int(d[p]) + w == int(d[q])
