@@ -244,6 +244,41 @@ int32_t pcbg_spec_add_history(pcbg_spec* s, float inc);
 /* 1 if a path through these board states would invalidate a search of net's window, else 0. */
 int32_t pcbg_spec_window_reads(pcbg_spec* s, int32_t net, const uint32_t* states, int32_t m);
 
+/* The engine's nets, board size and cost board (for schedulers). */
+int pcbg_spec_net(pcbg_spec* s, int32_t k, pcbg_net* out);
+void pcbg_spec_board(pcbg_spec* s, int32_t* nx, int32_t* ny, int32_t* nl);
+int pcbg_spec_costs(pcbg_spec* s, pcbg_costs** costs, int32_t* cls);
+
+/* ---- the learned speculation scheduler (no reference counterpart) --------------------------------------------
+ * A conflict predictor: a 3-layer MLP (PCBG_SCHED_FEATURES -> 128 -> 128 -> 1, BF16 operands, FP32 accumulation)
+ * over per-pair features of (searched net i, earlier uncommitted net j): 32 x 32 occupancy and history rasters of
+ * j's window, an 8 x 8 mask of i's window in it, and 64 box-overlap / pin scalars. Attached to a pcbg_spec it
+ * searches net i with the others of the window only while 1 - prod_j (1 - p_ij) < threshold; the plain batching is
+ * its fallback. Attached as a logger to plain rounds it records the features of every speculative pair; after the
+ * round pcbg_sched_label sets each pair's label (did j's committed path cross a block of i's window) and
+ * pcbg_sched_train fits the network on the GPU with its own forward / backward kernels and Adam. */
+#define PCBG_SCHED_FEATURES 2176
+#define PCBG_SCHED_HIDDEN 128
+typedef struct pcbg_sched pcbg_sched;
+pcbg_sched* pcbg_sched_create(uint64_t seed);
+void pcbg_sched_destroy(pcbg_sched* s);
+void pcbg_sched_attach(pcbg_sched* s, pcbg_spec* spec, float threshold);
+void pcbg_sched_attach_logger(pcbg_sched* s, pcbg_spec* spec);
+/* Labels of the pairs logged since the last call, from spec's committed paths; returns the positives. */
+int64_t pcbg_sched_label(pcbg_sched* s, pcbg_spec* spec);
+int64_t pcbg_sched_log_size(pcbg_sched* s, int64_t* positives);
+int pcbg_sched_train(pcbg_sched* s, int32_t epochs, float lr, int32_t batch, uint64_t seed, float* loss);
+void pcbg_sched_counts(pcbg_sched* s, int64_t* scored, int64_t* deferred);
+/* The network on host arrays. Parameters are packed f32: W1 [128][2176], W2 [128][128], b1, b2, w3 [128], b3.
+ * x: B rows of 2176 bf16 bit patterns, B a multiple of 64. */
+int64_t pcbg_sched_nparams(pcbg_sched* s);
+int pcbg_sched_get_params(pcbg_sched* s, float* out);
+int pcbg_sched_set_params(pcbg_sched* s, const float* in);
+int pcbg_sched_forward_host(pcbg_sched* s, const uint16_t* x, int32_t B, float* p);
+/* Gradients of sum_b w_b BCE(z_b, y_b) / sum_b w_b, packed like the parameters, and that loss. */
+int pcbg_sched_grad_host(pcbg_sched* s, const uint16_t* x, const float* y, const float* w, int32_t B, float* grad,
+                         float* loss);
+
 /* ---- seeded synthetic search generator (the batched-search microbenchmark workload) ----------------------- */
 
 /* Fill a pitched search with the seeded workload: per (layer, cell) cost 1 + (h % 16), about 15 % of cells

@@ -17,7 +17,10 @@ PCBG_SYMBOLS = [
     "pcbg_available", "pcbg_configure", "pcbg_solve", "pcbg_host_acquire", "pcbg_host_release", "pcbg_last_error",
     "pcbg_solve_batch", "pcbg_solve_noalloc", "pcbg_batch_window", "pcbg_batcher_stats", "pcbg_spec_create",
     "pcbg_spec_destroy", "pcbg_spec_set_scheduler", "pcbg_spec_set_observer", "pcbg_spec_iterate", "pcbg_spec_path",
-    "pcbg_spec_add_history", "pcbg_spec_window_reads", "pcbg_last_batch_tile_visits", "pcbg_last_batch_layer_visits", "pcbg_last_batch_rounds",
+    "pcbg_spec_add_history", "pcbg_spec_window_reads", "pcbg_spec_net", "pcbg_spec_board", "pcbg_spec_costs",
+    "pcbg_sched_create", "pcbg_sched_destroy", "pcbg_sched_attach", "pcbg_sched_attach_logger", "pcbg_sched_label",
+    "pcbg_sched_log_size", "pcbg_sched_train", "pcbg_sched_counts", "pcbg_sched_nparams", "pcbg_sched_get_params",
+    "pcbg_sched_set_params", "pcbg_sched_forward_host", "pcbg_sched_grad_host", "pcbg_last_batch_tile_visits", "pcbg_last_batch_layer_visits", "pcbg_last_batch_rounds",
     "pcbg_last_batch_kernel_ms", "pcbg_last_batch_launches", "pcbg_last_batch_local_iters", "pcbg_synth_search",
     "pcbg_synth_search_host", "pcbg_costs_create", "pcbg_costs_destroy", "pcbg_costs_set_static",
     "pcbg_costs_set_occupancy", "pcbg_costs_set_history", "pcbg_costs_set_ground", "pcbg_costs_rebuild",
@@ -146,6 +149,39 @@ def load() -> C.CDLL:
     lib.pcbg_spec_add_history.restype = C.c_int32
     lib.pcbg_spec_window_reads.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32]
     lib.pcbg_spec_window_reads.restype = C.c_int32
+    lib.pcbg_sched_create.argtypes = [C.c_uint64]
+    lib.pcbg_sched_create.restype = C.c_void_p
+    lib.pcbg_sched_destroy.argtypes = [C.c_void_p]
+    lib.pcbg_sched_destroy.restype = None
+    lib.pcbg_sched_attach.argtypes = [C.c_void_p, C.c_void_p, C.c_float]
+    lib.pcbg_sched_attach.restype = None
+    lib.pcbg_sched_attach_logger.argtypes = [C.c_void_p, C.c_void_p]
+    lib.pcbg_sched_attach_logger.restype = None
+    lib.pcbg_sched_label.argtypes = [C.c_void_p, C.c_void_p]
+    lib.pcbg_sched_label.restype = C.c_int64
+    lib.pcbg_sched_log_size.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+    lib.pcbg_sched_log_size.restype = C.c_int64
+    lib.pcbg_sched_train.argtypes = [C.c_void_p, C.c_int32, C.c_float, C.c_int32, C.c_uint64, C.POINTER(C.c_float)]
+    lib.pcbg_sched_train.restype = C.c_int
+    lib.pcbg_sched_counts.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    lib.pcbg_sched_counts.restype = None
+    lib.pcbg_sched_nparams.argtypes = [C.c_void_p]
+    lib.pcbg_sched_nparams.restype = C.c_int64
+    lib.pcbg_sched_get_params.argtypes = [C.c_void_p, C.c_void_p]
+    lib.pcbg_sched_get_params.restype = C.c_int
+    lib.pcbg_sched_set_params.argtypes = [C.c_void_p, C.c_void_p]
+    lib.pcbg_sched_set_params.restype = C.c_int
+    lib.pcbg_sched_forward_host.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]
+    lib.pcbg_sched_forward_host.restype = C.c_int
+    lib.pcbg_sched_grad_host.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
+                                         C.POINTER(C.c_float)]
+    lib.pcbg_sched_grad_host.restype = C.c_int
+    lib.pcbg_spec_net.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
+    lib.pcbg_spec_net.restype = C.c_int
+    lib.pcbg_spec_board.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.pcbg_spec_board.restype = None
+    lib.pcbg_spec_costs.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.pcbg_spec_costs.restype = C.c_int
     lib.pcbg_batch_window.argtypes = [C.c_int32]
     lib.pcbg_batch_window.restype = None
     lib.pcbg_batcher_stats.argtypes = [C.POINTER(C.c_int64), C.POINTER(C.c_int64)]

@@ -1,0 +1,426 @@
+// The learned speculation scheduler: a conflict predictor that picks which nets of the lookahead window are searched
+// together, so that fewer speculative searches are thrown away at the fixed-order commit.
+//
+// A speculative search of net i is wasted when a net j committed before it, and not yet committed when i was
+// searched, lays its path through a block of i's window (the acceptance test of src/router.cpp:2211-2216). The
+// predictor estimates that event per pair (i, j) from:
+//   * 32 x 32 rasters of j's window, sampled from the board as it is at the search: the occupancy (tracks and vias,
+//     all layers) and the history (all layers);
+//   * an 8 x 8 mask of where i's window lies within j's window;
+//   * 64 scalars of box overlap and pin geometry (overlap fractions, how much of j's pin-to-pin segment crosses i's
+//     window, pin positions, sizes, order gap, occupancy and history inside the overlap).
+// Net i's risk is 1 - prod_j (1 - p_ij) over the uncommitted nets before it; the scheduler searches i now when the
+// risk is below a threshold, otherwise it waits until those nets are committed. The net at the commit point is always
+// searched, and the commit order and acceptance test are untouched, so the paths do not change.
+//
+// Conflict logs: attached as an observer to plain speculative rounds, the scheduler records the features of every
+// (searched net, earlier uncommitted net) pair at search time; after the round the labels come from the committed
+// paths. Training runs the MLP's own forward and backward kernels (mlp.cu) with Adam, on the GPU.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "pcbg_internal.h"
+
+namespace pcbg {
+namespace {
+
+struct PairDesc {
+    int ix0, iy0, ix1, iy1;     // window of the searched net i
+    int jx0, jy0, jx1, jy1;     // window of the earlier net j
+    float jsx, jsy, jtx, jty;   // j's pins
+    float gap;                  // i - j
+};
+
+constexpr int RS = 32;   // raster side
+constexpr int MS = 8;    // mask side
+
+// One block per pair: features into X[pair][MLP_D0] (bf16).
+__global__ void __launch_bounds__(256) pair_features_kernel(CostPlanes P, const PairDesc* pd, __nv_bfloat16* X) {
+    const PairDesc d = pd[blockIdx.x];
+    __nv_bfloat16* x = X + size_t(blockIdx.x) * MLP_D0;
+    __shared__ float red[4][256];
+    const float jw = float(d.jx1 - d.jx0), jh = float(d.jy1 - d.jy0);
+    float so = 0.f, sh = 0.f, sio = 0.f, sih = 0.f;   // sums over the raster, and over its part inside i's window
+    for (int k = threadIdx.x; k < RS * RS; k += blockDim.x) {
+        const int u = k % RS, v = k / RS;
+        const int cx = min(d.jx1 - 1, d.jx0 + int((u + 0.5f) * jw / RS));
+        const int cy = min(d.jy1 - 1, d.jy0 + int((v + 0.5f) * jh / RS));
+        const size_t c = size_t(cy) * P.nx + cx;
+        float occ = 0.f, hs = 0.f;
+        for (int l = 0; l < P.nl; ++l) {
+            occ += float(P.oc[l][c]) + float(P.ov[l][c]);
+            hs += P.hist[l][c];
+        }
+        const float fo = fminf(occ, 8.f) * 0.25f, fh = fminf(hs / float(P.nl), 16.f) * 0.25f;
+        x[k] = __float2bfloat16_rn(fo);
+        x[RS * RS + k] = __float2bfloat16_rn(fh);
+        so += fo;
+        sh += fh;
+        if (cx >= d.ix0 && cx < d.ix1 && cy >= d.iy0 && cy < d.iy1) {
+            sio += fo;
+            sih += fh;
+        }
+    }
+    if (threadIdx.x < MS * MS) {
+        const int u = threadIdx.x % MS, v = threadIdx.x / MS;
+        const float cx = d.jx0 + (u + 0.5f) * jw / MS, cy = d.jy0 + (v + 0.5f) * jh / MS;
+        const bool in = cx >= d.ix0 && cx < d.ix1 && cy >= d.iy0 && cy < d.iy1;
+        x[2 * RS * RS + threadIdx.x] = __float2bfloat16_rn(in ? 1.f : 0.f);
+    }
+    red[0][threadIdx.x] = so;
+    red[1][threadIdx.x] = sh;
+    red[2][threadIdx.x] = sio;
+    red[3][threadIdx.x] = sih;
+    __syncthreads();
+    for (int o = 128; o; o >>= 1) {
+        if (threadIdx.x < o)
+            for (int r = 0; r < 4; ++r) red[r][threadIdx.x] += red[r][threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x < 64) {
+        const int f = threadIdx.x;
+        const float ox0 = fmaxf(d.ix0, d.jx0), ox1 = fminf(d.ix1, d.jx1), oy0 = fmaxf(d.iy0, d.jy0), oy1 = fminf(d.iy1, d.jy1);
+        const float ow = fmaxf(0.f, ox1 - ox0), oh = fmaxf(0.f, oy1 - oy0), oa = ow * oh;
+        const float ia = float(d.ix1 - d.ix0) * float(d.iy1 - d.iy0), ja = jw * jh;
+        // j's pin-to-pin segment against i's window, 64 samples
+        int inside = 0;
+        float dmin = 1e30f;
+        const float icx = 0.5f * (d.ix0 + d.ix1), icy = 0.5f * (d.iy0 + d.iy1);
+        for (int s = 0; s < 64; ++s) {
+            const float t = (s + 0.5f) / 64.f;
+            const float px = d.jsx + t * (d.jtx - d.jsx), py = d.jsy + t * (d.jty - d.jsy);
+            inside += (px >= d.ix0 && px < d.ix1 && py >= d.iy0 && py < d.iy1);
+            dmin = fminf(dmin, sqrtf((px - icx) * (px - icx) + (py - icy) * (py - icy)));
+        }
+        const float idiag = sqrtf(ia) + 1.f;
+        const float seg = sqrtf((d.jtx - d.jsx) * (d.jtx - d.jsx) + (d.jty - d.jsy) * (d.jty - d.jsy));
+        const bool sin_ = d.jsx >= d.ix0 && d.jsx < d.ix1 && d.jsy >= d.iy0 && d.jsy < d.iy1;
+        const bool tin = d.jtx >= d.ix0 && d.jtx < d.ix1 && d.jty >= d.iy0 && d.jty < d.iy1;
+        const float nin = fmaxf(1.f, oa / fmaxf(ja, 1.f) * RS * RS);
+        float v = 0.f;
+        switch (f) {
+            case 0: v = oa / fmaxf(ia, 1.f); break;
+            case 1: v = oa / fmaxf(ja, 1.f); break;
+            case 2: v = inside / 64.f; break;
+            case 3: v = inside > 0 ? 1.f : 0.f; break;
+            case 4: v = sin_ ? 1.f : 0.f; break;
+            case 5: v = tin ? 1.f : 0.f; break;
+            case 6: v = fminf(dmin / idiag, 4.f); break;
+            case 7: v = log2f(fmaxf(ia, 1.f)) / 16.f; break;
+            case 8: v = log2f(fmaxf(ja, 1.f)) / 16.f; break;
+            case 9: v = fminf(d.gap, 64.f) / 32.f; break;
+            case 10: v = red[2][0] / nin; break;
+            case 11: v = red[3][0] / nin; break;
+            case 12: v = red[0][0] / (RS * RS); break;
+            case 13: v = red[1][0] / (RS * RS); break;
+            case 14: v = fminf(seg, 512.f) / 128.f; break;
+            case 15: v = 1.f; break;
+            case 16: v = (d.jsx - icx) / idiag; break;
+            case 17: v = (d.jsy - icy) / idiag; break;
+            case 18: v = (d.jtx - icx) / idiag; break;
+            case 19: v = (d.jty - icy) / idiag; break;
+            default: v = 0.f;
+        }
+        x[2 * RS * RS + MS * MS + f] = __float2bfloat16_rn(v);
+    }
+}
+
+// rows idx[0..n) of X into Y (n rows), zero rows up to m
+__global__ void gather_rows_kernel(const __nv_bfloat16* X, const int* idx, int n, int m, __nv_bfloat16* Y) {
+    const int r = blockIdx.x;
+    const uint4 z = make_uint4(0, 0, 0, 0);
+    const uint4* src = r < n ? reinterpret_cast<const uint4*>(X + size_t(idx[r]) * MLP_D0) : nullptr;
+    uint4* dst = reinterpret_cast<uint4*>(Y + size_t(r) * MLP_D0);
+    for (int k = threadIdx.x; k < MLP_D0 / 8; k += blockDim.x) dst[k] = src ? src[k] : z;
+    (void)m;
+}
+
+}  // namespace
+}  // namespace pcbg
+
+using namespace pcbg;
+
+struct pcbg_sched {
+    Mlp net;
+    cudaStream_t stream = nullptr;
+    float threshold = 0.5f;
+    // conflict log: features on the device, pair geometry and labels on the host
+    __nv_bfloat16* X = nullptr;
+    size_t xcap = 0, nlog = 0;
+    std::vector<int> li, lj;        // logged pairs (net i searched, earlier net j), in log order
+    std::vector<float> label;       // 0 / 1, filled by pcbg_sched_label (NaN until then)
+    size_t labelled = 0;
+    // scratch
+    PairDesc* pd = nullptr;
+    size_t pdcap = 0;
+    __nv_bfloat16* xb = nullptr;    // a batch of features
+    size_t xbcap = 0;
+    float *yb = nullptr, *wb = nullptr, *pb = nullptr;
+    int* ib = nullptr;
+    size_t ybcap = 0, wbcap = 0, pbcap = 0, ibcap = 0;
+    int64_t scored = 0, deferred = 0;
+};
+
+namespace {
+
+template <class T> bool grow(T*& p, size_t& cap, size_t n) {
+    if (cap >= n) return true;
+    const size_t c = std::max(n, cap * 2);
+    T* q = nullptr;
+    if (cudaMalloc(&q, c * sizeof(T)) != cudaSuccess) return false;
+    if (p) {
+        cudaMemcpy(q, p, cap * sizeof(T), cudaMemcpyDeviceToDevice);
+        cudaFree(p);
+    }
+    p = q;
+    cap = c;
+    return true;
+}
+
+bool pair_of(pcbg_spec* s, int i, int j, int nx, PairDesc& d) {
+    pcbg_net a, b;
+    if (pcbg_spec_net(s, i, &a) != 0 || pcbg_spec_net(s, j, &b) != 0) return false;
+    d.ix0 = a.x0; d.iy0 = a.y0; d.ix1 = a.x1; d.iy1 = a.y1;
+    d.jx0 = b.x0; d.jy0 = b.y0; d.jx1 = b.x1; d.jy1 = b.y1;
+    int32_t nxv = 0, nyv = 0;
+    pcbg_spec_board(s, &nxv, &nyv, nullptr);
+    const size_t board = size_t(nxv) * nyv;
+    const int sc = int(b.src % board), tc = int(b.tgt % board);
+    d.jsx = float(sc % nx); d.jsy = float(sc / nx);
+    d.jtx = float(tc % nx); d.jty = float(tc / nx);
+    d.gap = float(i - j);
+    return true;
+}
+
+// features of pairs into X rows [row0, row0 + n)
+int features(pcbg_sched* S, pcbg_spec* s, const std::vector<PairDesc>& pds, __nv_bfloat16* X) {
+    if (pds.empty()) return 0;
+    CostPlanes P;
+    pcbg_costs* costs = nullptr;
+    int32_t cls = 0;
+    if (pcbg_spec_costs(s, &costs, &cls) != 0 || !cost_planes(costs, cls, P)) return -1;
+    if (!grow(S->pd, S->pdcap, pds.size())) return -1;
+    cudaMemcpyAsync(S->pd, pds.data(), pds.size() * sizeof(PairDesc), cudaMemcpyHostToDevice, S->stream);
+    pair_features_kernel<<<unsigned(pds.size()), 256, 0, S->stream>>>(P, S->pd, X);
+    if (cudaGetLastError() != cudaSuccess) return -1;
+    return cudaStreamSynchronize(S->stream) == cudaSuccess ? 0 : -1;
+}
+
+int sched_pick(void* user, pcbg_spec* s, int32_t cursor, const int32_t* cand, int32_t n, int32_t* pick) {
+    pcbg_sched* S = static_cast<pcbg_sched*>(user);
+    int32_t nx = 0, ny = 0;
+    pcbg_spec_board(s, &nx, &ny, nullptr);
+    std::vector<PairDesc> pds;
+    std::vector<int> owner;
+    for (int k = 0; k < n; ++k) {
+        const int i = cand[k];
+        for (int j = cursor; j < i; ++j) {
+            PairDesc d;
+            if (!pair_of(s, i, j, nx, d)) return -1;
+            pds.push_back(d);
+            owner.push_back(k);
+        }
+    }
+    for (int k = 0; k < n; ++k) pick[k] = cand[k] == cursor ? 1 : 0;
+    if (pds.empty()) return 0;
+    const size_t B = round_up(pds.size(), 64);
+    if (!grow(S->xb, S->xbcap, B * MLP_D0) || !grow(S->pb, S->pbcap, B)) return -1;
+    cudaMemsetAsync(S->xb, 0, B * MLP_D0 * 2, S->stream);
+    if (features(S, s, pds, S->xb) != 0) return -1;
+    if (S->net.forward(S->stream, S->xb, int(B), S->pb) != 0) return -1;
+    std::vector<float> p(pds.size());
+    cudaMemcpyAsync(p.data(), S->pb, p.size() * 4, cudaMemcpyDeviceToHost, S->stream);
+    if (cudaStreamSynchronize(S->stream) != cudaSuccess) return -1;
+    std::vector<double> keep(n, 1.0);
+    for (size_t q = 0; q < pds.size(); ++q) keep[owner[q]] *= 1.0 - double(p[q]);
+    for (int k = 0; k < n; ++k) {
+        if (cand[k] == cursor) continue;
+        ++S->scored;
+        if (1.0 - keep[k] < double(S->threshold)) pick[k] = 1;
+        else ++S->deferred;
+    }
+    return 0;
+}
+
+void sched_log(void* user, pcbg_spec* s, int32_t cursor, int32_t net) {
+    pcbg_sched* S = static_cast<pcbg_sched*>(user);
+    if (net <= cursor) return;
+    int32_t nx = 0, ny = 0;
+    pcbg_spec_board(s, &nx, &ny, nullptr);
+    std::vector<PairDesc> pds;
+    for (int j = cursor; j < net; ++j) {
+        PairDesc d;
+        if (!pair_of(s, net, j, nx, d)) return;
+        pds.push_back(d);
+        S->li.push_back(net);
+        S->lj.push_back(j);
+        S->label.push_back(std::nanf(""));
+    }
+    if (!grow(S->X, S->xcap, (S->nlog + pds.size()) * MLP_D0)) {
+        set_error("conflict log allocation failed");
+        S->li.resize(S->nlog); S->lj.resize(S->nlog); S->label.resize(S->nlog);
+        return;
+    }
+    if (features(S, s, pds, S->X + S->nlog * MLP_D0) != 0) {
+        S->li.resize(S->nlog); S->lj.resize(S->nlog); S->label.resize(S->nlog);
+        return;
+    }
+    S->nlog += pds.size();
+}
+
+}  // namespace
+
+extern "C" pcbg_sched* pcbg_sched_create(uint64_t seed) {
+    pcbg_sched* S = new pcbg_sched();
+    if (!S->net.init(seed) || cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete S;
+        set_error("scheduler allocation failed");
+        return nullptr;
+    }
+    return S;
+}
+
+extern "C" void pcbg_sched_destroy(pcbg_sched* S) {
+    if (!S) return;
+    cudaStreamSynchronize(S->stream);
+    for (void* p : {static_cast<void*>(S->X), static_cast<void*>(S->pd), static_cast<void*>(S->xb),
+                    static_cast<void*>(S->yb), static_cast<void*>(S->wb), static_cast<void*>(S->pb),
+                    static_cast<void*>(S->ib)})
+        if (p) cudaFree(p);
+    cudaStreamDestroy(S->stream);
+    delete S;
+}
+
+extern "C" void pcbg_sched_attach(pcbg_sched* S, pcbg_spec* s, float threshold) {
+    S->threshold = threshold;
+    pcbg_spec_set_scheduler(s, sched_pick, S);
+}
+
+extern "C" void pcbg_sched_attach_logger(pcbg_sched* S, pcbg_spec* s) { pcbg_spec_set_observer(s, sched_log, S); }
+
+extern "C" int64_t pcbg_sched_label(pcbg_sched* S, pcbg_spec* s) {
+    int64_t pos = 0;
+    std::vector<std::vector<uint32_t>> paths;
+    for (size_t q = S->labelled; q < S->nlog; ++q) {
+        const int j = S->lj[q];
+        const int32_t n = pcbg_spec_path(s, j, nullptr, 0);
+        std::vector<uint32_t> p(std::max(n, 0));
+        if (n > 0) pcbg_spec_path(s, j, p.data(), n);
+        const int32_t r = pcbg_spec_window_reads(s, S->li[q], p.data(), int32_t(p.size()));
+        if (r < 0) return PCBG_ERR_FAIL;
+        S->label[q] = float(r);
+        pos += r;
+    }
+    S->labelled = S->nlog;
+    return pos;
+}
+
+extern "C" int64_t pcbg_sched_log_size(pcbg_sched* S, int64_t* positives) {
+    int64_t p = 0;
+    for (size_t q = 0; q < S->labelled; ++q) p += S->label[q] > 0.5f;
+    if (positives) *positives = p;
+    return int64_t(S->labelled);
+}
+
+extern "C" int pcbg_sched_train(pcbg_sched* S, int32_t epochs, float lr, int32_t batch, uint64_t seed, float* loss_out) {
+    const size_t n = S->labelled;
+    if (n == 0 || batch < 64 || batch % 64) { set_error("nothing labelled, or batch not a multiple of 64"); return PCBG_ERR_FAIL; }
+    if (!grow(S->xb, S->xbcap, size_t(batch) * MLP_D0) || !grow(S->yb, S->ybcap, size_t(batch)) ||
+        !grow(S->wb, S->wbcap, size_t(batch)) || !grow(S->ib, S->ibcap, size_t(batch)))
+        return PCBG_ERR_FAIL;
+    // positives and negatives weighted to equal total weight
+    size_t npos = 0;
+    for (size_t q = 0; q < n; ++q) npos += S->label[q] > 0.5f;
+    const float wpos = npos ? float(n) / (2.f * npos) : 1.f, wneg = npos < n ? float(n) / (2.f * (n - npos)) : 1.f;
+    std::vector<int> order(n);
+    std::iota(order.begin(), order.end(), 0);
+    uint64_t st = seed;
+    auto rnd = [&]() {
+        st = st * 6364136223846793005ull + 1442695040888963407ull;
+        return st >> 33;
+    };
+    float last = 0.f;
+    std::vector<float> y(batch), w(batch);
+    for (int e = 0; e < epochs; ++e) {
+        for (size_t k = n - 1; k > 0; --k) std::swap(order[k], order[rnd() % (k + 1)]);
+        double esum = 0.0;
+        int nb = 0;
+        for (size_t b0 = 0; b0 < n; b0 += size_t(batch)) {
+            const int m = int(std::min<size_t>(batch, n - b0));
+            float wsum = 0.f;
+            for (int r = 0; r < batch; ++r) {
+                if (r < m) {
+                    const float lab = S->label[order[b0 + r]];
+                    y[r] = lab;
+                    w[r] = lab > 0.5f ? wpos : wneg;
+                    wsum += w[r];
+                } else {
+                    y[r] = 0.f;
+                    w[r] = 0.f;
+                }
+            }
+            cudaMemcpyAsync(S->ib, order.data() + b0, size_t(m) * 4, cudaMemcpyHostToDevice, S->stream);
+            cudaMemcpyAsync(S->yb, y.data(), size_t(batch) * 4, cudaMemcpyHostToDevice, S->stream);
+            cudaMemcpyAsync(S->wb, w.data(), size_t(batch) * 4, cudaMemcpyHostToDevice, S->stream);
+            gather_rows_kernel<<<batch, 128, 0, S->stream>>>(S->X, S->ib, m, batch, S->xb);
+            float loss = 0.f;
+            if (S->net.forward(S->stream, S->xb, batch, nullptr) != 0) return PCBG_ERR_FAIL;
+            if (S->net.backward(S->stream, S->xb, S->yb, S->wb, wsum, batch, &loss) != 0) return PCBG_ERR_FAIL;
+            if (S->net.adam(S->stream, lr) != 0) return PCBG_ERR_FAIL;
+            if (cudaStreamSynchronize(S->stream) != cudaSuccess) return PCBG_ERR_FAIL;
+            esum += loss;
+            ++nb;
+        }
+        last = float(esum / std::max(nb, 1));
+    }
+    if (loss_out) *loss_out = last;
+    return 0;
+}
+
+extern "C" void pcbg_sched_counts(pcbg_sched* S, int64_t* scored, int64_t* deferred) {
+    if (scored) *scored = S->scored;
+    if (deferred) *deferred = S->deferred;
+}
+
+// ---- host-array entry points of the network (the gradient check against the CPU oracle) ----
+
+extern "C" int64_t pcbg_sched_nparams(pcbg_sched* S) { return int64_t(S->net.nparams); }
+
+extern "C" int pcbg_sched_get_params(pcbg_sched* S, float* out) {
+    return cudaMemcpy(out, S->net.master, S->net.nparams * 4, cudaMemcpyDeviceToHost) == cudaSuccess ? 0 : PCBG_ERR_FAIL;
+}
+
+extern "C" int pcbg_sched_set_params(pcbg_sched* S, const float* in) { return S->net.set_params(in) == 0 ? 0 : PCBG_ERR_FAIL; }
+
+/* x: B rows of MLP_D0 bf16 bit patterns (B a multiple of 64). p: B probabilities. */
+extern "C" int pcbg_sched_forward_host(pcbg_sched* S, const uint16_t* x, int32_t B, float* p) {
+    if (B <= 0 || B % 64 || !grow(S->xb, S->xbcap, size_t(B) * MLP_D0) || !grow(S->pb, S->pbcap, size_t(B))) return PCBG_ERR_FAIL;
+    cudaMemcpyAsync(S->xb, x, size_t(B) * MLP_D0 * 2, cudaMemcpyHostToDevice, S->stream);
+    if (S->net.forward(S->stream, S->xb, B, S->pb) != 0) return PCBG_ERR_FAIL;
+    cudaMemcpyAsync(p, S->pb, size_t(B) * 4, cudaMemcpyDeviceToHost, S->stream);
+    return cudaStreamSynchronize(S->stream) == cudaSuccess ? 0 : PCBG_ERR_FAIL;
+}
+
+/* Gradients (packed like the parameters) of sum_b w_b BCE(z_b, y_b) / sum_b w_b, and that loss. */
+extern "C" int pcbg_sched_grad_host(pcbg_sched* S, const uint16_t* x, const float* y, const float* w, int32_t B,
+                                    float* grad, float* loss) {
+    if (B <= 0 || B % 64) return PCBG_ERR_FAIL;
+    if (!grow(S->xb, S->xbcap, size_t(B) * MLP_D0) || !grow(S->yb, S->ybcap, size_t(B)) || !grow(S->wb, S->wbcap, size_t(B)))
+        return PCBG_ERR_FAIL;
+    float* yd = S->yb;
+    float* wd = S->wb;
+    float wsum = 0.f;
+    for (int b = 0; b < B; ++b) wsum += w[b];
+    cudaMemcpyAsync(S->xb, x, size_t(B) * MLP_D0 * 2, cudaMemcpyHostToDevice, S->stream);
+    cudaMemcpyAsync(yd, y, size_t(B) * 4, cudaMemcpyHostToDevice, S->stream);
+    cudaMemcpyAsync(wd, w, size_t(B) * 4, cudaMemcpyHostToDevice, S->stream);
+    int rc = S->net.forward(S->stream, S->xb, B, nullptr);
+    if (rc == 0) rc = S->net.backward(S->stream, S->xb, yd, wd, wsum, B, loss);
+    if (rc == 0 && cudaMemcpyAsync(grad, S->net.grad, S->net.nparams * 4, cudaMemcpyDeviceToHost, S->stream) != cudaSuccess) rc = -1;
+    if (cudaStreamSynchronize(S->stream) != cudaSuccess) rc = -1;
+    return rc == 0 ? 0 : PCBG_ERR_FAIL;
+}

@@ -429,3 +429,22 @@ extern "C" int32_t pcbg_spec_window_reads(pcbg_spec* S, int32_t net, const uint3
     std::vector<uint32_t> p(states, states + m);
     return window_reads(S, S->nets[net], blocks_of(S, p)) ? 1 : 0;
 }
+
+extern "C" int pcbg_spec_net(pcbg_spec* S, int32_t k, pcbg_net* out) {
+    if (!S || k < 0 || k >= int32_t(S->nets.size())) return PCBG_ERR_FAIL;
+    *out = S->nets[k];
+    return 0;
+}
+
+extern "C" void pcbg_spec_board(pcbg_spec* S, int32_t* nx, int32_t* ny, int32_t* nl) {
+    if (nx) *nx = S->P.nx;
+    if (ny) *ny = S->P.ny;
+    if (nl) *nl = S->P.nl;
+}
+
+extern "C" int pcbg_spec_costs(pcbg_spec* S, pcbg_costs** costs, int32_t* cls) {
+    if (!S) return PCBG_ERR_FAIL;
+    *costs = S->costs;
+    *cls = S->cls;
+    return 0;
+}
