@@ -215,6 +215,7 @@ typedef struct pcbg_spec_stats {
     int64_t conflicts;          /* nets whose path shares a state with another net's path */
     double search_ms;           /* host time in the batched searches (resolve, launch, walk-back, paths read) */
     double total_ms;
+    double relax_ms;            /* device time of the relaxation launches (CUDA events) */
 } pcbg_spec_stats;
 
 typedef struct pcbg_spec pcbg_spec;

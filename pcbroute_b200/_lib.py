@@ -97,7 +97,8 @@ class Net(C.Structure):
 class SpecStats(C.Structure):
     """struct pcbg_spec_stats."""
     _fields_ = [("searches", C.c_int64), ("wasted", C.c_int64), ("batches", C.c_int64), ("commits", C.c_int64),
-                ("conflicts", C.c_int64), ("search_ms", C.c_double), ("total_ms", C.c_double)]
+                ("conflicts", C.c_int64), ("search_ms", C.c_double), ("total_ms", C.c_double),
+                ("relax_ms", C.c_double)]
 
 
 SCHEDULER = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.c_int32,

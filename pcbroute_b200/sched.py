@@ -122,3 +122,78 @@ def run(b: dict, iters: int, width: int, sch: Scheduler | None = None, threshold
         return r.paths(), stats
     finally:
         r.close()
+
+
+def ab_report(train_seeds, test_seeds, board_kw: dict, iters: int = 3, width: int = 16, epochs: int = 12,
+              threshold: float = 0.5, seed: int = 21) -> dict:
+    """Train on the conflict logs of plain rounds over `train_seeds` boards, then negotiate the `test_seeds` boards
+    sequentially (one search per launch), with the plain batching and with the learned one. Returns the totals per
+    method (searches, wasted searches, launches, host and device milliseconds) and whether all three committed the
+    same paths."""
+    import time
+    train = [spec.spec_board(s, **board_kw) for s in train_seeds]
+    test = [spec.spec_board(s, **board_kw) for s in test_seeds]
+    sch = Scheduler(seed)
+    t0 = time.time()
+    collect_logs(sch, train, iters=iters, width=width)
+    n, pos = sch.log_size()
+    t1 = time.time()
+    loss = sch.train(epochs=epochs)
+    t2 = time.time()
+    out = {"train_boards": len(train), "test_boards": len(test), "board": board_kw, "iters": iters, "width": width,
+           "log_pairs": n, "log_positives": pos, "train_loss": round(loss, 4), "log_s": round(t1 - t0, 2),
+           "train_s": round(t2 - t1, 2), "threshold": threshold}
+    ref = {}
+    same = True
+    for name, pol, s in (("sequential", spec.SEQUENTIAL, None), ("plain", spec.PLAIN, None),
+                         ("learned", spec.LEARNED, sch)):
+        tot = dict(searches=0, wasted=0, batches=0, total_ms=0.0, search_ms=0.0, relax_ms=0.0)
+        for b in test:
+            r = spec.Round(b)
+            try:
+                if s is not None:
+                    s.attach(r, threshold)
+                for it in range(iters):
+                    st = r.iterate(spec.pres_of(it), pol, width)
+                    for k in tot:
+                        tot[k] += st[k]
+                    if it + 1 < iters:
+                        r.add_history(1.0)
+                paths = r.paths()
+            finally:
+                r.close()
+            if name == "sequential":
+                ref[b["seed"]] = paths
+            else:
+                same &= all(np.array_equal(a, c) for a, c in zip(ref[b["seed"]], paths))
+        tot["wasted_fraction"] = round(tot["wasted"] / max(1, tot["searches"]), 4)
+        for k in ("total_ms", "search_ms", "relax_ms"):
+            tot[k] = round(tot[k], 1)
+        out[name] = tot
+    out["identical_paths"] = bool(same)
+    sch.close()
+    return out
+
+
+def main() -> None:
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="learned vs plain speculative batching on seeded boards (A/B)")
+    ap.add_argument("--train", type=int, default=8)
+    ap.add_argument("--test", type=int, default=4)
+    ap.add_argument("--nx", type=int, default=320)
+    ap.add_argument("--ny", type=int, default=256)
+    ap.add_argument("--nl", type=int, default=6)
+    ap.add_argument("--nets", type=int, default=160)
+    ap.add_argument("--iters", type=int, default=3)
+    ap.add_argument("--width", type=int, default=16)
+    ap.add_argument("--epochs", type=int, default=12)
+    ap.add_argument("--threshold", type=float, default=0.5)
+    a = ap.parse_args()
+    kw = dict(nx=a.nx, ny=a.ny, nl=a.nl, nnets=a.nets, margin=12, span=(16, max(24, min(a.nx, a.ny) // 2)))
+    r = ab_report(range(100, 100 + a.train), range(900, 900 + a.test), kw, a.iters, a.width, a.epochs, a.threshold)
+    print(json.dumps(r))
+
+
+if __name__ == "__main__":
+    main()
