@@ -130,6 +130,25 @@ def cost_map_roofline(lib, peak):
             "frac": round(ach / peak, 4), "algorithmic_bytes": alg}
 
 
+def learned_batching():
+    """The speculative negotiation rounds on seeded 320 x 256 x 6 boards of 160 nets: the conflict predictor trained
+    on the logs of plain rounds over 4 boards, then 3 rip-up-and-reroute iterations on 2 held-out boards with one
+    search per launch (sequential), the plain batching (lookahead 16) and the learned batching. Host time of the
+    rounds (searches, walk-backs, commits), the wasted-search fraction, and whether all three committed the same
+    paths."""
+    from pcbroute_b200 import sched
+    kw = dict(nx=320, ny=256, nl=6, nnets=160, margin=12, span=(16, 128))
+    r = sched.ab_report(range(100, 104), range(900, 902), kw, iters=3, width=16, epochs=12)
+    out = {"workload": "2 held-out seeded boards 320x256x6, 160 two-pin nets, 3 iterations; predictor trained on "
+                       "the conflict logs of 4 other boards",
+           "identical_paths": r["identical_paths"], "log_pairs": r["log_pairs"], "train_s": r["train_s"]}
+    for k in ("sequential", "plain", "learned"):
+        out[k] = {x: r[k][x] for x in ("total_ms", "relax_ms", "searches", "wasted", "wasted_fraction", "batches")}
+    out["speedup_learned_vs_sequential"] = round(r["sequential"]["total_ms"] / r["learned"]["total_ms"], 3)
+    out["speedup_learned_vs_plain"] = round(r["plain"]["total_ms"] / r["learned"]["total_ms"], 3)
+    return out
+
+
 def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -216,6 +235,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--no-spec", action="store_true", help="skip the learned-vs-plain speculative batching A/B")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -345,32 +365,58 @@ def main():
         d2h = [sum(x.numel() * 4 for x in oh) for oh in outs_h]
         e_states = [sum(s["rw"] * s["rh"] * s["nl"] for s in w) for w in ew]
 
-        def e2e_step(k):
+        # Steps are pipelined the way a caller with two wave buffers would run them: the inputs of step k+1 go up
+        # on one copy stream and the fields of step k come down on another while step k+1's launch runs. Every
+        # step still moves its own inputs in and its own fields out inside the timed region.
+        cs_in, cs_out = torch.cuda.Stream(), torch.cuda.Stream()
+        ev_in = [torch.cuda.Event() for _ in ew]
+        ev_out = [torch.cuda.Event() for _ in ew]
+
+        def e2e_h2d(k):
             i = k % len(ew)
-            for s, (hc, hf, hv) in zip(ew[i], host_in[i]):
-                s["cf"].copy_(hc, non_blocking=True)
-                s["fl"].copy_(hf, non_blocking=True)
-                s["vcf"].copy_(hv, non_blocking=True)
+            with torch.cuda.stream(cs_in):
+                for s, (hc, hf, hv) in zip(ew[i], host_in[i]):
+                    s["cf"].copy_(hc, non_blocking=True)
+                    s["fl"].copy_(hf, non_blocking=True)
+                    s["vcf"].copy_(hv, non_blocking=True)
+                ev_in[i].record(cs_in)
+
+        def e2e_solve(k):
+            i = k % len(ew)
+            stream.wait_event(ev_in[i])      # this step's inputs are up
+            stream.wait_event(ev_out[i])     # the fields of the wave that used these buffers before are down
             arr, _ = e_arrays[i]
             if lib.pcbg_solve_batch(arr, len(arr), sp) != 0:
                 raise RuntimeError("pcbg_solve_batch failed: " + _lib.last_error())
-            for od, oh in zip(outs_d[i], outs_h[i]):
-                oh.copy_(od, non_blocking=True)
-            return e_states[i], h2d[i], d2h[i], lib.pcbg_last_batch_launches()
+            cs_out.wait_stream(stream)
+            with torch.cuda.stream(cs_out):
+                for od, oh in zip(outs_d[i], outs_h[i]):
+                    oh.copy_(od, non_blocking=True)
+                ev_out[i].record(cs_out)
+            return e_states[i], h2d[i], d2h[i]
 
-        for k in range(min(args.warmup, 2)):
-            e2e_step(k)
+        def e2e_run(n):
+            es = eb_in = eb_out = 0
+            cs_in.wait_stream(stream)        # the first upload starts after the timing event
+            e2e_h2d(0)
+            for k in range(n):
+                if k + 1 < n:
+                    e2e_h2d(k + 1)
+                a, b, c = e2e_solve(k)
+                es += a
+                eb_in += b
+                eb_out += c
+            for e in ev_out:
+                stream.wait_event(e)
+            return es, eb_in, eb_out
+
+        e2e_run(min(args.warmup, 2))
         torch.cuda.synchronize()
         barrier()
         torch.cuda.synchronize()
         f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        es, eb_in, eb_out = 0, 0, 0
         f0.record(stream)
-        for k in range(args.steps):
-            a, b, c, _ = e2e_step(k)
-            es += a
-            eb_in += b
-            eb_out += c
+        es, eb_in, eb_out = e2e_run(args.steps)
         f1.record(stream)
         torch.cuda.synchronize()
         barrier()
@@ -381,7 +427,8 @@ def main():
             dist.all_reduce(etot, op=dist.ReduceOp.SUM)
         e2e = {"value": round(9.0 * float(etot.item()) / (float(et.item()) / 1e3) / 1e9, 4), "unit": UNIT,
                "h2d_bytes_per_step": int(eb_in // args.steps), "d2h_bytes_per_step": int(eb_out // args.steps),
-               "waves": len(ew), "api": "pcbg_solve_batch from pinned host buffers, reported fields read back"}
+               "waves": len(ew), "api": "pcbg_solve_batch from pinned host buffers, reported fields read back; "
+                                              "copies of neighbouring steps overlap the launch on two copy streams"}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -412,6 +459,7 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "cost_maps": cost_map_roofline(lib, peak),
+            "learned_batching": None if args.no_spec else learned_batching(),
             "e2e": e2e,
             "cpu_baseline": cpu,
         }

@@ -148,6 +148,9 @@ struct Mlp {
     int adam(cudaStream_t s, float lr);
 };
 
+// Side of the square cell blocks by which speculative rounds track what a search read and a commit changed.
+constexpr int SPEC_BLOCK = 8;
+
 inline size_t round_up(size_t x, size_t m) { return (x + m - 1) / m * m; }
 
 }  // namespace pcbg

@@ -173,6 +173,7 @@ template <class T> bool grow(T*& p, size_t& cap, size_t n) {
     T* q = nullptr;
     if (cudaMalloc(&q, c * sizeof(T)) != cudaSuccess) return false;
     if (p) {
+        cudaDeviceSynchronize();   // kernels still writing the old buffer run on non-blocking streams
         cudaMemcpy(q, p, cap * sizeof(T), cudaMemcpyDeviceToDevice);
         cudaFree(p);
     }
@@ -196,7 +197,17 @@ bool pair_of(pcbg_spec* s, int i, int j, int nx, PairDesc& d) {
     return true;
 }
 
-// features of pairs into X rows [row0, row0 + n)
+// Whether net j's path can invalidate a search of net i at all: a path stays inside its own window, and a commit
+// invalidates i only through blocks of i's window, so pairs whose windows share no block never conflict.
+bool blocks_meet(pcbg_spec* s, int i, int j) {
+    pcbg_net a, b;
+    if (pcbg_spec_net(s, i, &a) != 0 || pcbg_spec_net(s, j, &b) != 0) return true;
+    const int B = SPEC_BLOCK;
+    return a.x0 / B <= (b.x1 - 1) / B && b.x0 / B <= (a.x1 - 1) / B && a.y0 / B <= (b.y1 - 1) / B &&
+           b.y0 / B <= (a.y1 - 1) / B;
+}
+
+// features of pairs into X rows [row0, row0 + n) (stream-ordered on the scheduler's stream)
 int features(pcbg_sched* S, pcbg_spec* s, const std::vector<PairDesc>& pds, __nv_bfloat16* X) {
     if (pds.empty()) return 0;
     CostPlanes P;
@@ -206,8 +217,7 @@ int features(pcbg_sched* S, pcbg_spec* s, const std::vector<PairDesc>& pds, __nv
     if (!grow(S->pd, S->pdcap, pds.size())) return -1;
     cudaMemcpyAsync(S->pd, pds.data(), pds.size() * sizeof(PairDesc), cudaMemcpyHostToDevice, S->stream);
     pair_features_kernel<<<unsigned(pds.size()), 256, 0, S->stream>>>(P, S->pd, X);
-    if (cudaGetLastError() != cudaSuccess) return -1;
-    return cudaStreamSynchronize(S->stream) == cudaSuccess ? 0 : -1;
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 int sched_pick(void* user, pcbg_spec* s, int32_t cursor, const int32_t* cand, int32_t n, int32_t* pick) {
@@ -219,6 +229,7 @@ int sched_pick(void* user, pcbg_spec* s, int32_t cursor, const int32_t* cand, in
     for (int k = 0; k < n; ++k) {
         const int i = cand[k];
         for (int j = cursor; j < i; ++j) {
+            if (!blocks_meet(s, i, j)) continue;   // p_ij = 0
             PairDesc d;
             if (!pair_of(s, i, j, nx, d)) return -1;
             pds.push_back(d);
@@ -226,7 +237,10 @@ int sched_pick(void* user, pcbg_spec* s, int32_t cursor, const int32_t* cand, in
         }
     }
     for (int k = 0; k < n; ++k) pick[k] = cand[k] == cursor ? 1 : 0;
-    if (pds.empty()) return 0;
+    if (pds.empty()) {   // no open net shares a block with an uncommitted one: all are safe
+        for (int k = 0; k < n; ++k) pick[k] = 1;
+        return 0;
+    }
     const size_t B = round_up(pds.size(), 64);
     if (!grow(S->xb, S->xbcap, B * MLP_D0) || !grow(S->pb, S->pbcap, B)) return -1;
     cudaMemsetAsync(S->xb, 0, B * MLP_D0 * 2, S->stream);
@@ -253,6 +267,7 @@ void sched_log(void* user, pcbg_spec* s, int32_t cursor, int32_t net) {
     pcbg_spec_board(s, &nx, &ny, nullptr);
     std::vector<PairDesc> pds;
     for (int j = cursor; j < net; ++j) {
+        if (!blocks_meet(s, net, j)) continue;   // never a conflict: not logged
         PairDesc d;
         if (!pair_of(s, net, j, nx, d)) return;
         pds.push_back(d);

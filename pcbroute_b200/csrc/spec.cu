@@ -29,7 +29,7 @@
 namespace pcbg {
 namespace {
 
-constexpr int BS = 8;   // cells per side of a touched block
+constexpr int BS = SPEC_BLOCK;   // cells per side of a touched block
 
 struct WinDesc {
     int x0, y0, rw, rh, pitch, hpad;
