@@ -109,12 +109,12 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cost_map_roofline(lib, peak):
+def cost_map_roofline(lib, peak, nx=5000, ny=4000):
     """Device rebuild of the congestion cost maps (rebuild_costs, src/router.cpp:409-420) on a board the size of the
     8-layer stress configuration: 5000 x 4000 cells, 8 layers, 4 net classes. Algorithmic bytes per rebuild: per
     class and layer st 2 + oc 1 + cst 4 per cell; per class vst 2 + 8 ov + vcst 4 per cell; the 8 history planes
     (4 B) once."""
-    nx, ny, nl, k = 5000, 4000, 8, 4
+    nl, k = 8, 4
     h = lib.pcbg_costs_create(nx, ny, nl, k)
     if not h:
         return None
@@ -125,7 +125,7 @@ def cost_map_roofline(lib, peak):
     n = nx * ny
     alg = k * (nl * n * 7 + n * (2 + nl + 4)) + nl * n * 4
     ach = alg / (ms / 1e3) / 1e9
-    return {"kernel": "costs_rebuild_kernel", "workload": "5000 x 4000 cells, 8 layers, 4 classes",
+    return {"kernel": "costs_rebuild_kernel", "workload": f"{nx} x {ny} cells, 8 layers, 4 classes",
             "ms": round(ms, 3), "bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
             "frac": round(ach / peak, 4), "algorithmic_bytes": alg}
 
@@ -236,6 +236,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-spec", action="store_true", help="skip the learned-vs-plain speculative batching A/B")
+    ap.add_argument("--cost-maps-only", type=int, nargs=2, metavar=("NX", "NY"), default=None,
+                    help="only time the cost-map rebuild on an NX x NY x 8 board of 4 classes (a profiling case)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -251,6 +253,10 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     lib = _lib.load()
+    if args.cost_maps_only:
+        if rank == 0:
+            print(json.dumps(cost_map_roofline(lib, peaks()[0], *args.cost_maps_only)))
+        return
     if not lib.pcbg_available():
         raise RuntimeError("B200 back end unavailable: " + _lib.last_error())
     stream = torch.cuda.current_stream()

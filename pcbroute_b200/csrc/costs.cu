@@ -71,62 +71,89 @@ __device__ __forceinline__ float cost_via(const CostDev& D, int k, size_t c, flo
     return s == FREE ? v : -v;
 }
 
-// every cell of every class: 8 cells per thread (128-bit loads of st/hist/gnd and stores of cst)
-__global__ void costs_rebuild_kernel(CostDev D, float pres, int hard) {
+// via cost of one cell from its summed history and via occupancy (src/router.cpp:396-405 with own = 0)
+__device__ __forceinline__ float via_of(uint16_t s, int occ, float a, float pres, int hard) {
+    if (s == BLOCK) return CINF;
+    if (hard && occ > 0) return CINF;
+    const float v = __fmul_rn(a, __fadd_rn(1.f, __fmul_rn(pres, float(occ > 0 ? occ : 0))));
+    return s == FREE ? v : -v;
+}
+
+// Every cell of every class, 4 cells per thread and one pass: the history of every layer is loaded once (128-bit)
+// and serves both the track costs of its layer and the via costs' layer sum. Per class, the owners (64-bit, 4
+// cells) and occupancy (32-bit, 4 cells) of every layer and the via grids are loaded before any cost is computed,
+// so a thread keeps them all in flight at once. The history sum runs in layer order, as vcost_xp does.
+__global__ void __launch_bounds__(256) costs_rebuild_kernel(CostDev D, float pres, int hard) {
     const size_t n = size_t(D.n);
-    const size_t groups = (n + 7) / 8;
-    for (size_t g = size_t(blockIdx.x) * blockDim.x + threadIdx.x; g < groups * D.nl; g += size_t(gridDim.x) * blockDim.x) {
-        const int l = int(g / groups);
-        const size_t c0 = (g % groups) * 8;
-        const bool full = c0 + 8 <= n;
-        float h[8], gf[8];
-        if (full) {
-            const float4* hp = reinterpret_cast<const float4*>(D.hist[l] + c0);
-            const float4 h0 = hp[0], h1 = hp[1];
-            h[0] = h0.x; h[1] = h0.y; h[2] = h0.z; h[3] = h0.w; h[4] = h1.x; h[5] = h1.y; h[6] = h1.z; h[7] = h1.w;
-        } else {
-            for (int e = 0; e < 8; ++e) h[e] = c0 + e < n ? D.hist[l][c0 + e] : 0.f;
-        }
-        for (int k = 0; k < D.nclasses; ++k) {
-            const int id = k * MAX_LAYERS + l;
-            float out[8];
-            if (full) {
-                const uint4 sv = *reinterpret_cast<const uint4*>(D.st[id] + c0);
-                const uint2 ov = *reinterpret_cast<const uint2*>(D.oc[id] + c0);
-                const uint16_t s[8] = {uint16_t(sv.x), uint16_t(sv.x >> 16), uint16_t(sv.y), uint16_t(sv.y >> 16),
-                                       uint16_t(sv.z), uint16_t(sv.z >> 16), uint16_t(sv.w), uint16_t(sv.w >> 16)};
-                const uint8_t o[8] = {uint8_t(ov.x), uint8_t(ov.x >> 8), uint8_t(ov.x >> 16), uint8_t(ov.x >> 24),
-                                      uint8_t(ov.y), uint8_t(ov.y >> 8), uint8_t(ov.y >> 16), uint8_t(ov.y >> 24)};
-                #pragma unroll
-                for (int e = 0; e < 8; ++e) out[e] = cost_track(s[e], o[e], h[e], D.gnd[l], c0 + e, pres, hard);
-                float4* op = reinterpret_cast<float4*>(D.cst[id] + c0);
-                op[0] = make_float4(out[0], out[1], out[2], out[3]);
-                op[1] = make_float4(out[4], out[5], out[6], out[7]);
-            } else {
-                for (size_t c = c0; c < n; ++c)
-                    D.cst[id][c] = cost_track(D.st[id][c], D.oc[id][c], D.hist[l][c], D.gnd[l], c, pres, hard);
-            }
-        }
-        (void)gf;
-    }
-    // via maps: one cell per thread; the layer sum of the history is shared by the classes (summed in layer
-    // order, as vcost_xp does)
-    for (size_t c = size_t(blockIdx.x) * blockDim.x + threadIdx.x; c < n; c += size_t(gridDim.x) * blockDim.x) {
-        float hs = 0.f;
-        for (int l = 0; l < D.nl; ++l) hs = __fadd_rn(hs, D.hist[l][c]);
-        const float a = __fadd_rn(1.f, __fdiv_rn(hs, float(D.nl)));
-        for (int k = 0; k < D.nclasses; ++k) {
-            const uint16_t s = D.vst[k][c];
-            float v = CINF;
-            if (s != BLOCK) {
-                int occ = 0;
-                for (int l = 0; l < D.nl; ++l) occ += D.ov[k * MAX_LAYERS + l][c];
-                if (!(hard && occ > 0)) {
-                    v = __fmul_rn(a, __fadd_rn(1.f, __fmul_rn(pres, float(occ > 0 ? occ : 0))));
-                    if (s != FREE) v = -v;
+    const int nl = D.nl, nc = D.nclasses;
+    const size_t quads = (n + 3) / 4;
+    for (size_t q = size_t(blockIdx.x) * blockDim.x + threadIdx.x; q < quads; q += size_t(gridDim.x) * blockDim.x) {
+        const size_t c0 = q * 4;
+        if (c0 + 4 > n) {   // ragged end of the board
+            for (size_t c = c0; c < n; ++c) {
+                float hsum = 0.f;
+                for (int l = 0; l < nl; ++l) hsum = __fadd_rn(hsum, D.hist[l][c]);
+                const float a = __fadd_rn(1.f, __fdiv_rn(hsum, float(nl)));
+                for (int k = 0; k < nc; ++k) {
+                    int occ = 0;
+                    for (int l = 0; l < nl; ++l) {
+                        const int id = k * MAX_LAYERS + l;
+                        D.cst[id][c] = cost_track(D.st[id][c], D.oc[id][c], D.hist[l][c], D.gnd[l], c, pres, hard);
+                        occ += D.ov[id][c];
+                    }
+                    D.vcst[k][c] = via_of(D.vst[k][c], occ, a, pres, hard);
                 }
             }
-            D.vcst[k][c] = v;
+            continue;
+        }
+        float4 hv[MAX_LAYERS];
+        #pragma unroll
+        for (int l = 0; l < MAX_LAYERS; ++l)
+            if (l < nl) hv[l] = __ldcs(reinterpret_cast<const float4*>(D.hist[l] + c0));
+        float hs[4] = {0.f, 0.f, 0.f, 0.f};
+        #pragma unroll
+        for (int l = 0; l < MAX_LAYERS; ++l)
+            if (l < nl) {
+                hs[0] = __fadd_rn(hs[0], hv[l].x);
+                hs[1] = __fadd_rn(hs[1], hv[l].y);
+                hs[2] = __fadd_rn(hs[2], hv[l].z);
+                hs[3] = __fadd_rn(hs[3], hv[l].w);
+            }
+        float a[4];
+        #pragma unroll
+        for (int e = 0; e < 4; ++e) a[e] = __fadd_rn(1.f, __fdiv_rn(hs[e], float(nl)));
+        for (int k = 0; k < nc; ++k) {
+            uint2 sv[MAX_LAYERS];
+            uint32_t oc[MAX_LAYERS], ow[MAX_LAYERS];
+            #pragma unroll
+            for (int l = 0; l < MAX_LAYERS; ++l)
+                if (l < nl) {
+                    const int id = k * MAX_LAYERS + l;
+                    sv[l] = __ldcs(reinterpret_cast<const uint2*>(D.st[id] + c0));
+                    oc[l] = __ldcs(reinterpret_cast<const uint32_t*>(D.oc[id] + c0));
+                    ow[l] = __ldcs(reinterpret_cast<const uint32_t*>(D.ov[id] + c0));
+                }
+            const uint2 vv = __ldcs(reinterpret_cast<const uint2*>(D.vst[k] + c0));
+            int occ[4] = {0, 0, 0, 0};
+            #pragma unroll
+            for (int l = 0; l < MAX_LAYERS; ++l)
+                if (l < nl) {
+                    const float h[4] = {hv[l].x, hv[l].y, hv[l].z, hv[l].w};
+                    const uint16_t st[4] = {uint16_t(sv[l].x), uint16_t(sv[l].x >> 16), uint16_t(sv[l].y), uint16_t(sv[l].y >> 16)};
+                    const uint8_t o[4] = {uint8_t(oc[l]), uint8_t(oc[l] >> 8), uint8_t(oc[l] >> 16), uint8_t(oc[l] >> 24)};
+                    float out[4];
+                    #pragma unroll
+                    for (int e = 0; e < 4; ++e) out[e] = cost_track(st[e], o[e], h[e], D.gnd[l], c0 + e, pres, hard);
+                    __stcs(reinterpret_cast<float4*>(D.cst[k * MAX_LAYERS + l] + c0), make_float4(out[0], out[1], out[2], out[3]));
+                    occ[0] += int(ow[l] & 0xFF);
+                    occ[1] += int((ow[l] >> 8) & 0xFF);
+                    occ[2] += int((ow[l] >> 16) & 0xFF);
+                    occ[3] += int(ow[l] >> 24);
+                }
+            const uint16_t vs[4] = {uint16_t(vv.x), uint16_t(vv.x >> 16), uint16_t(vv.y), uint16_t(vv.y >> 16)};
+            __stcs(reinterpret_cast<float4*>(D.vcst[k] + c0),
+                   make_float4(via_of(vs[0], occ[0], a[0], pres, hard), via_of(vs[1], occ[1], a[1], pres, hard),
+                               via_of(vs[2], occ[2], a[2], pres, hard), via_of(vs[3], occ[3], a[3], pres, hard)));
         }
     }
 }
