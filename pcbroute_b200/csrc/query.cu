@@ -116,7 +116,28 @@ struct Slot {
     DBuf<int> pcol, prow;
     DBuf<float> mlf;
     DBuf<uint32_t> lidx, sidx;
+    unsigned char* stage = nullptr;   // pinned host staging of a rectangle's cost maps
+    size_t stage_cap = 0;
 };
+
+// Grow-only pinned staging buffer of a slot.
+bool stage_need(Slot& E, size_t n) {
+    if (E.stage_cap >= n) return true;
+    if (E.stage) cudaFreeHost(E.stage);
+    E.stage = nullptr;
+    E.stage_cap = 0;
+    const size_t c = n + n / 4 + 4096;
+    if (cudaHostAlloc(reinterpret_cast<void**>(&E.stage), c, cudaHostAllocDefault) != cudaSuccess) { E.stage = nullptr; return false; }
+    E.stage_cap = c;
+    return true;
+}
+
+// Rows [y0, y0 + rh) x columns [x0, x0 + rw) of a row-major host grid of row length nx, packed with row pitch
+// `pitch` into dst.
+template <class T>
+void pack_rows(T* dst, const T* src, size_t nx, size_t hoff, int rw, int rh, int pitch) {
+    for (int j = 0; j < rh; ++j) memcpy(dst + size_t(j) * pitch, src + hoff + size_t(j) * nx, size_t(rw) * sizeof(T));
+}
 
 std::mutex g_cfg_mu;
 int g_slots = 4;
@@ -176,15 +197,23 @@ int solve_rect(Slot& E, const pcbg_query& q, int rx0, int ry0, int rw, int rh, p
     }
     cudaStream_t S = E.stream;
     const size_t hoff = size_t(q.wj0 + ry0) * q.nx + (q.wi0 + rx0);
-    for (int l = 0; l < nl; ++l) {
-        CK(cudaMemcpy2DAsync(E.cf.p + size_t(l) * plane, size_t(pitch) * 4, q.cst[l] + hoff, size_t(q.nx) * 4, size_t(rw) * 4, rh,
-                             cudaMemcpyHostToDevice, S));
-        CK(cudaMemcpy2DAsync(E.st.p + size_t(l) * plane, size_t(pitch) * 2, q.st[l] + hoff, size_t(q.nx) * 2, size_t(rw) * 2, rh,
-                             cudaMemcpyHostToDevice, S));
-    }
-    if (vias) {
-        CK(cudaMemcpy2DAsync(E.vcf.p, size_t(pitch) * 4, q.vcst + hoff, size_t(q.nx) * 4, size_t(rw) * 4, rh, cudaMemcpyHostToDevice, S));
-        CK(cudaMemcpy2DAsync(E.vst.p, size_t(pitch) * 2, q.vst + hoff, size_t(q.nx) * 2, size_t(rw) * 2, rh, cudaMemcpyHostToDevice, S));
+    // The rectangle's rows of the host cost maps are packed into pinned staging, then copied with one DMA per grid:
+    // a strided copy from pageable memory moves row by row through the driver's own staging and runs several
+    // times slower. Rows keep the device pitch, so each grid is one contiguous copy (padding cells are written by
+    // the resolve kernel).
+    const size_t rows = size_t(rh) * pitch;
+    const size_t grid_bytes = rows * 6, total = grid_bytes * size_t(nl + (vias ? 1 : 0));
+    if (!stage_need(E, total)) { set_error("pinned allocation failed"); return -1; }
+    for (int l = 0; l <= nl; ++l) {
+        if (l == nl && !vias) break;
+        float* hc = reinterpret_cast<float*>(E.stage + size_t(l) * grid_bytes);
+        uint16_t* hs = reinterpret_cast<uint16_t*>(E.stage + size_t(l) * grid_bytes + rows * 4);
+        pack_rows(hc, l < nl ? q.cst[l] : q.vcst, size_t(q.nx), hoff, rw, rh, pitch);
+        pack_rows(hs, l < nl ? q.st[l] : q.vst, size_t(q.nx), hoff, rw, rh, pitch);
+        float* dc = l < nl ? E.cf.p + size_t(l) * plane : E.vcf.p;
+        uint16_t* ds = l < nl ? E.st.p + size_t(l) * plane : E.vst.p;
+        CK(cudaMemcpyAsync(dc, hc, rows * 4, cudaMemcpyHostToDevice, S));
+        CK(cudaMemcpyAsync(ds, hs, rows * 2, cudaMemcpyHostToDevice, S));
     }
     if (q.prior) {
         CK(cudaMemcpyAsync(E.pcol.p, q.pcol + q.wi0 + rx0, size_t(rw) * 4, cudaMemcpyHostToDevice, S));
