@@ -130,6 +130,26 @@ def cost_map_roofline(lib, peak, nx=5000, ny=4000):
             "frac": round(ach / peak, 4), "algorithmic_bytes": alg}
 
 
+def plain_gpu_comparison(n=48):
+    """The one-search gpu_solve path of pcbroute's own CUDA back end (src/gpu.cu for sm_100a, built unchanged by
+    baseline/Makefile) against this library's, on the first n searches of this workload from dense host arrays
+    (upload, solve and field download in each timed call). Runs baseline/plain_gpu.py once per arm, each in its own
+    process. None when the reference back end has not been built here."""
+    if not os.path.exists(os.path.join(ROOT, "baseline", "_ref", "librefgpu.so")):
+        return None
+    out = {}
+    for arm in ("ref", "b200"):
+        r = subprocess.run([sys.executable, os.path.join(ROOT, "baseline", "plain_gpu.py"), "--arm", arm,
+                            "--searches", str(n)], capture_output=True, text=True, timeout=900)
+        if r.returncode != 0:
+            return {"error": f"{arm}: " + r.stderr[-300:]}
+        out[arm] = json.loads(r.stdout.strip().splitlines()[-1])
+    return {"workload": f"first {n} searches of this workload, one gpu_solve call each from host arrays",
+            "plain_gpu_gcell_relax_s": out["ref"]["gcell_relax_s"], "b200_gcell_relax_s": out["b200"]["gcell_relax_s"],
+            "plain_gpu_seconds": out["ref"]["seconds"], "b200_seconds": out["b200"]["seconds"],
+            "speedup_one_search_path": round(out["ref"]["seconds"] / out["b200"]["seconds"], 2)}
+
+
 def learned_batching():
     """The speculative negotiation rounds on seeded 320 x 256 x 6 boards of 160 nets: the conflict predictor trained
     on the logs of plain rounds over 4 boards, then 3 rip-up-and-reroute iterations on 2 held-out boards with one
@@ -466,6 +486,7 @@ def main():
             "clocks": clk.summary(),
             "cost_maps": cost_map_roofline(lib, peak),
             "learned_batching": None if args.no_spec else learned_batching(),
+            "plain_gpu": None if args.no_spec else plain_gpu_comparison(),
             "e2e": e2e,
             "cpu_baseline": cpu,
         }
