@@ -265,7 +265,7 @@ def main():
 
     import torch
     import torch.distributed as dist
-    from pcbroute_b200 import _lib, synth
+    from pcbroute_b200 import _lib, replicas, synth
 
     ws, rank, local = dist_setup()
     torch.cuda.set_device(local)
@@ -285,7 +285,7 @@ def main():
     sizes = synth.microbench_sizes(SEED, args.searches)
     waves = [sizes[i:i + args.wave] for i in range(0, len(sizes), args.wave)]
     nw = len(waves)
-    my = [waves[(rank + ws * k) % nw] for k in range(max(1, -(-nw // ws)))]
+    my = replicas.my_waves(waves, ws, rank)
 
     # generate every search of my waves on the device (pitched layout), once
     def make(sz):
@@ -363,12 +363,7 @@ def main():
     barrier()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    tot = torch.tensor([float(st_done)], dtype=torch.float64, device="cuda")
-    if ws > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
-    ms_max, states_all = float(t.item()), float(tot.item())
+    ms_max, states_all = replicas.max_time_sum_work(ms, st_done, "cuda", ws)
     value = 9.0 * states_all / (ms_max / 1e3) / 1e9
     alg_bytes = lv * BYTES_PER_LAYER_VISIT + tv * BYTES_PER_TILE_VISIT
     peak, peak_kind = peaks()
@@ -446,12 +441,8 @@ def main():
         f1.record(stream)
         torch.cuda.synchronize()
         barrier()
-        et = torch.tensor([f0.elapsed_time(f1)], dtype=torch.float64, device="cuda")
-        etot = torch.tensor([float(es)], dtype=torch.float64, device="cuda")
-        if ws > 1:
-            dist.all_reduce(et, op=dist.ReduceOp.MAX)
-            dist.all_reduce(etot, op=dist.ReduceOp.SUM)
-        e2e = {"value": round(9.0 * float(etot.item()) / (float(et.item()) / 1e3) / 1e9, 4), "unit": UNIT,
+        et, etot = replicas.max_time_sum_work(f0.elapsed_time(f1), es, "cuda", ws)
+        e2e = {"value": round(9.0 * etot / (et / 1e3) / 1e9, 4), "unit": UNIT,
                "h2d_bytes_per_step": int(eb_in // args.steps), "d2h_bytes_per_step": int(eb_out // args.steps),
                "waves": len(ew), "api": "pcbg_solve_batch from pinned host buffers, reported fields read back; "
                                               "copies of neighbouring steps overlap the launch on two copy streams"}
