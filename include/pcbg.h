@@ -162,8 +162,10 @@ int64_t pcbg_last_batch_local_iters(void);   /* sum over tile visits of local re
  * pcbg_solve / gpu_solve calls that run concurrently, from the router's worker threads (src/router.cpp:2187-2235
  * runs T of them ahead of the commit point), are solved together: each prepares its inputs on its own slot
  * stream, then the searches queued at that moment run in one persistent relaxation launch. The leader waits for
- * searches still preparing at most `us` microseconds (default 2000; 0: never waits). Results never depend on the
- * grouping. pcbg_batcher_stats reports the launches made and the searches they solved since the library loaded. */
+ * searches still preparing at most a window that tunes itself between 50 and 2000 microseconds: waits that bring no
+ * search in shrink it, waits that do widen it. pcbg_batch_window(us) fixes it at `us` (0: never wait); a negative
+ * value returns to the tuned window. Results never depend on the grouping. pcbg_batcher_stats reports the launches
+ * made and the searches they solved since the library loaded. */
 void pcbg_batch_window(int32_t us);
 void pcbg_batcher_stats(int64_t* batches, int64_t* searches);
 

@@ -10,6 +10,7 @@
 //
 // Results do not depend on the grouping. Every search has its own distance field, worklists and bound in the batch,
 // and the field is the exact least fixed point, whatever the schedule.
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <mutex>
@@ -34,8 +35,19 @@ struct Batcher {
     int preparing = 0;             // searches that will submit soon
     cudaStream_t stream = nullptr;
     long long batches = 0, searches = 0;
-    int window_us = 2000;
+    int window_us = 2000;          // current wait limit of a leader
+    int cap_us = 2000;             // its upper limit
+    bool adaptive = true;          // tune window_us from what the waits bring in
 } g_b;
+
+// The batching window tunes itself: a leader whose whole wait brought no other search in shrinks it (x0.7, down to
+// 50 us), since the searches still preparing were too far from submitting; a wait that did bring searches in
+// widens it (x1.25, up to the cap). A wait that ended because nobody was preparing any more leaves it as it is.
+void tune_window(bool timed_out, size_t before, size_t after) {
+    if (!g_b.adaptive) return;
+    if (timed_out && after == before) g_b.window_us = std::max(50, int(g_b.window_us * 0.7));
+    else if (after > before) g_b.window_us = std::min(g_b.cap_us, int(g_b.window_us * 1.25) + 1);
+}
 
 }  // namespace
 
@@ -63,8 +75,10 @@ int batcher_submit(BatchItem& item, BatchResult& res) {
         }
         // lead: wait for the searches still preparing their inputs, at most the batching window
         g_b.leading = true;
+        const size_t before = g_b.queue.size();
         const auto until = std::chrono::steady_clock::now() + std::chrono::microseconds(g_b.window_us);
-        g_b.cv.wait_until(lk, until, [] { return g_b.preparing <= 0; });
+        const bool ready = g_b.cv.wait_until(lk, until, [] { return g_b.preparing <= 0; });
+        tune_window(!ready, before, g_b.queue.size());
         std::vector<Ticket*> take;
         take.swap(g_b.queue);
         if (!g_b.stream && cudaStreamCreateWithFlags(&g_b.stream, cudaStreamNonBlocking) != cudaSuccess) g_b.stream = nullptr;
@@ -96,7 +110,12 @@ int batcher_submit(BatchItem& item, BatchResult& res) {
 
 void batcher_window(int us) {
     std::lock_guard<std::mutex> g(g_b.mu);
-    g_b.window_us = us < 0 ? 0 : us;
+    if (us < 0) {           // tuned between 50 us and the cap
+        g_b.adaptive = true;
+        return;
+    }
+    g_b.adaptive = false;   // fixed
+    g_b.window_us = us;
 }
 
 void batcher_stats(long long* batches, long long* searches) {

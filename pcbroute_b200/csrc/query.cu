@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "pcbg_internal.h"
@@ -135,8 +136,8 @@ bool stage_need(Slot& E, size_t n) {
 // Rows [y0, y0 + rh) x columns [x0, x0 + rw) of a row-major host grid of row length nx, packed with row pitch
 // `pitch` into dst.
 template <class T>
-void pack_rows(T* dst, const T* src, size_t nx, size_t hoff, int rw, int rh, int pitch) {
-    for (int j = 0; j < rh; ++j) memcpy(dst + size_t(j) * pitch, src + hoff + size_t(j) * nx, size_t(rw) * sizeof(T));
+void pack_rows(T* dst, const T* src, size_t nx, size_t hoff, int rw, int j0, int j1, int pitch) {
+    for (int j = j0; j < j1; ++j) memcpy(dst + size_t(j) * pitch, src + hoff + size_t(j) * nx, size_t(rw) * sizeof(T));
 }
 
 std::mutex g_cfg_mu;
@@ -204,12 +205,28 @@ int solve_rect(Slot& E, const pcbg_query& q, int rx0, int ry0, int rw, int rh, p
     const size_t rows = size_t(rh) * pitch;
     const size_t grid_bytes = rows * 6, total = grid_bytes * size_t(nl + (vias ? 1 : 0));
     if (!stage_need(E, total)) { set_error("pinned allocation failed"); return -1; }
-    for (int l = 0; l <= nl; ++l) {
-        if (l == nl && !vias) break;
+    const int ngrids = nl + (vias ? 1 : 0);
+    auto pack = [&](int j0, int j1) {
+        for (int l = 0; l < ngrids; ++l) {
+            pack_rows(reinterpret_cast<float*>(E.stage + size_t(l) * grid_bytes), l < nl ? q.cst[l] : q.vcst,
+                      size_t(q.nx), hoff, rw, j0, j1, pitch);
+            pack_rows(reinterpret_cast<uint16_t*>(E.stage + size_t(l) * grid_bytes + rows * 4), l < nl ? q.st[l] : q.vst,
+                      size_t(q.nx), hoff, rw, j0, j1, pitch);
+        }
+    };
+    // a whole-board rectangle packs tens of MB: split its rows over a few threads
+    const int nth = total > (size_t(16) << 20) ? 4 : 1;
+    if (nth == 1) {
+        pack(0, rh);
+    } else {
+        std::vector<std::thread> th;
+        for (int t = 1; t < nth; ++t) th.emplace_back(pack, rh * t / nth, rh * (t + 1) / nth);
+        pack(0, rh / nth);
+        for (auto& x : th) x.join();
+    }
+    for (int l = 0; l < ngrids; ++l) {
         float* hc = reinterpret_cast<float*>(E.stage + size_t(l) * grid_bytes);
         uint16_t* hs = reinterpret_cast<uint16_t*>(E.stage + size_t(l) * grid_bytes + rows * 4);
-        pack_rows(hc, l < nl ? q.cst[l] : q.vcst, size_t(q.nx), hoff, rw, rh, pitch);
-        pack_rows(hs, l < nl ? q.st[l] : q.vst, size_t(q.nx), hoff, rw, rh, pitch);
         float* dc = l < nl ? E.cf.p + size_t(l) * plane : E.vcf.p;
         uint16_t* ds = l < nl ? E.st.p + size_t(l) * plane : E.vst.p;
         CK(cudaMemcpyAsync(dc, hc, rows * 4, cudaMemcpyHostToDevice, S));
