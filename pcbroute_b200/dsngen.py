@@ -100,6 +100,16 @@ CONFIGS = {
     "c2": Config("c2", 100, 80, ["F.Cu", "In1.Cu", "In2.Cu", "B.Cu"],
                  [("QFP100", 1), ("R0402", 20), ("R0603", 20), ("SOIC8", 12)], 300, 500, 0.2, (3, 6),
                  [("default", 200, 150, 0.85), ("power", 400, 250, 0.15)], [("GND", "In1.Cu"), ("VCC", "In2.Cu")]),
+    # 6 layers, BGA-256 at 1.0 mm pitch + 150 passives (+ SOIC-8s for pins), up to 1200 nets / 2000 connections as
+    # the pins allow, 20 % multi-pin (3-6), two classes
+    "c4": Config("c4", 160, 100, ["F.Cu", "In1.Cu", "In2.Cu", "In3.Cu", "In4.Cu", "B.Cu"],
+                 [("BGA256", 2), ("R0402", 75), ("R0603", 75), ("SOIC8", 120)], 1200, 2000, 0.2, (3, 6),
+                 [("default", 200, 150, 0.85), ("power", 400, 250, 0.15)]),
+    # 8 layers, 250 x 200 mm, up to 3000 nets / 6000 connections as the pins allow, four classes
+    "c5": Config("c5", 250, 200, ["F.Cu", "In1.Cu", "In2.Cu", "In3.Cu", "In4.Cu", "In5.Cu", "In6.Cu", "B.Cu"],
+                 [("BGA256", 4), ("R0402", 300), ("R0603", 300), ("SOIC8", 300)], 3000, 6000, 0.3, (3, 6),
+                 [("default", 150, 150, 0.6), ("signal", 200, 150, 0.2), ("power", 400, 250, 0.15),
+                  ("hv", 500, 400, 0.05)], [("GND", "In1.Cu"), ("VCC", "In6.Cu")]),
     # small boards for the parity tests
     "t1": Config("t1", 24, 18, ["F.Cu", "B.Cu"], [("SOIC8", 3), ("R0805", 4)], 10, 14),
     "t2": Config("t2", 30, 24, ["F.Cu", "In1.Cu", "In2.Cu", "B.Cu"], [("SOIC8", 4), ("R0603", 6)], 16, 24, 0.2, (3, 4),
