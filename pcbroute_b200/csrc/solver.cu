@@ -180,43 +180,104 @@ __device__ __forceinline__ void side_lines(unsigned sides, uint32_t (&w)[6]) {
 
 // ---- staging shared by both modes ----
 
+// Staging is latency-bound: a visit's loads come from L2 or HBM, and a block has few warps. Each thread therefore
+// issues a whole chunk of independent loads before it stores any of them.
+constexpr int STAGE_CHUNK = 4;
+
 template <typename DT>
 __device__ void stage_dist(const SDev& S, DT* dS, int x0, int y0) {
     const DT* dist = reinterpret_cast<const DT*>(S.dist);
-    for (int idx = threadIdx.x; idx < S.nl * HS * HS; idx += NT) {
-        const int l = idx / (HS * HS), rem = idx % (HS * HS), r = rem / HS, c = rem % HS;
-        const int gy = y0 + r - 1, gx = x0 + c - 1;
-        DT v = Lim<DT>::INF;
-        // distances are written by other blocks during the launch: read them at L2, never from this SM's L1
-        if (gy >= 0 && gy < S.hpad && gx >= 0 && gx < S.pitch) v = __ldcg(dist + (size_t(l) * S.hpad + gy) * S.pitch + gx);
-        dS[l * LS + r * DSTR + c] = v;
+    const int total = S.nl * HS * HS;
+    for (int base = threadIdx.x; base < total; base += NT * STAGE_CHUNK) {
+        DT v[STAGE_CHUNK];
+        #pragma unroll
+        for (int u = 0; u < STAGE_CHUNK; ++u) {
+            const int idx = base + u * NT;
+            const int l = idx / (HS * HS), rem = idx % (HS * HS), r = rem / HS, c = rem % HS;
+            const int gy = y0 + r - 1, gx = x0 + c - 1;
+            v[u] = Lim<DT>::INF;
+            // distances are written by other blocks during the launch: read them at L2, never from this SM's L1
+            if (idx < total && gy >= 0 && gy < S.hpad && gx >= 0 && gx < S.pitch)
+                v[u] = __ldcg(dist + (size_t(l) * S.hpad + gy) * S.pitch + gx);
+        }
+        #pragma unroll
+        for (int u = 0; u < STAGE_CHUNK; ++u) {
+            const int idx = base + u * NT;
+            if (idx >= total) break;
+            const int l = idx / (HS * HS), rem = idx % (HS * HS), r = rem / HS, c = rem % HS;
+            dS[l * LS + r * DSTR + c] = v[u];
+        }
     }
 }
 
-// via weight per cell and the via-landing / target layer masks
+// 32-bit distances: 16-byte loads. A staged row spans columns x0 - 1 .. x0 + 32; the aligned words x0 - 4 .. x0 + 35
+// cover it in 10 loads, and words outside the field (left of column 0, right of the pitch, rows off the field)
+// stay unreached.
+template <>
+__device__ void stage_dist<uint32_t>(const SDev& S, uint32_t* dS, int x0, int y0) {
+    const uint32_t* dist = reinterpret_cast<const uint32_t*>(S.dist);
+    constexpr int G = 10;   // 16-byte groups per staged row
+    const int total = S.nl * HS * G;
+    for (int base = threadIdx.x; base < total; base += NT * STAGE_CHUNK) {
+        uint4 v[STAGE_CHUNK];
+        #pragma unroll
+        for (int u = 0; u < STAGE_CHUNK; ++u) {
+            const int it = base + u * NT;
+            const int l = it / (HS * G), rem = it % (HS * G), r = rem / G, g = rem % G;
+            const int gy = y0 + r - 1, gx = x0 - 4 + 4 * g;
+            v[u] = make_uint4(INF32, INF32, INF32, INF32);
+            if (it < total && gy >= 0 && gy < S.hpad && gx >= 0 && gx + 4 <= S.pitch)
+                v[u] = __ldcg(reinterpret_cast<const uint4*>(dist + (size_t(l) * S.hpad + gy) * S.pitch + gx));
+        }
+        #pragma unroll
+        for (int u = 0; u < STAGE_CHUNK; ++u) {
+            const int it = base + u * NT;
+            if (it >= total) break;
+            const int l = it / (HS * G), rem = it % (HS * G), r = rem / G, g = rem % G;
+            const uint32_t w[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
+            #pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int c = 4 * g + e - 3;   // staged column: word x0 - 4 + 4g + e is column c - 1 of the tile
+                if (c >= 0 && c < HS) dS[l * LS + r * DSTR + c] = w[e];
+            }
+        }
+    }
+}
+
+// via weight per cell and the via-landing / target layer masks; 4 cells per thread-step (the flags of 4 cells are
+// one 32-bit word per layer, the via costs one 128-bit word), all layers' words loaded before any is used
 template <typename DT>
 __device__ void stage_cells(const SDev& S, DT* vS, uint32_t* vokS, uint32_t* tgS, int x0, int y0, bool& wide,
                             unsigned long long& wmax) {
-    for (int cell = threadIdx.x; cell < TILE * TILE; cell += NT) {
-        const int r = cell >> 5, c = cell & 31;
-        DT wv = Lim<DT>::INF;
-        if (S.vcf) {
-            const float v = S.vcf[size_t(y0 + r) * S.pitch + x0 + c];
+    for (int g = threadIdx.x; g < TILE * TILE / 4; g += NT) {
+        const int r = g >> 3, c0 = (g & 7) * 4;
+        uint32_t fw[MAX_LAYERS];
+        #pragma unroll
+        for (int l = 0; l < MAX_LAYERS; ++l)
+            fw[l] = l < S.nl ? *reinterpret_cast<const uint32_t*>(S.fl + (size_t(l) * S.hpad + y0 + r) * S.pitch + x0 + c0) : 0u;
+        float4 vv = make_float4(1e30f, 1e30f, 1e30f, 1e30f);
+        if (S.vcf) vv = *reinterpret_cast<const float4*>(S.vcf + size_t(y0 + r) * S.pitch + x0 + c0);
+        const float vc[4] = {vv.x, vv.y, vv.z, vv.w};
+        #pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            DT wv = Lim<DT>::INF;
+            const float v = vc[e];
             if (v < 1e30f) {
                 const float y = __fmul_rn(v, 16.0f);
                 if (!(y < Lim<DT>::wlim())) wide = true;
                 else { wv = qweight<DT>(v, 1.0f); wmax = max(wmax, static_cast<unsigned long long>(wv)); }
             }
+            vS[r * CSTR + c0 + e] = wv;
+            unsigned int vm = 0, tm = 0;
+            #pragma unroll
+            for (int l = 0; l < MAX_LAYERS; ++l) {
+                const unsigned f = (fw[l] >> (8 * e)) & 0xFFu;
+                vm |= (f & 1u) << l;
+                tm |= ((f >> 1) & 1u) << l;
+            }
+            vokS[r * CSTR + c0 + e] = vm;
+            tgS[r * CSTR + c0 + e] = tm;
         }
-        vS[r * CSTR + c] = wv;
-        unsigned int vm = 0, tm = 0;
-        for (int l = 0; l < S.nl; ++l) {
-            const uint8_t f = S.fl[(size_t(l) * S.hpad + y0 + r) * S.pitch + x0 + c];
-            vm |= unsigned(f & 1) << l;
-            tm |= unsigned((f >> 1) & 1) << l;
-        }
-        vokS[r * CSTR + c] = vm;
-        tgS[r * CSTR + c] = tm;
     }
 }
 
@@ -582,19 +643,39 @@ __device__ void visit_tile(const SolveArgs& a, int s, int tile, int round, unsig
             if (w >= 0xFFFFu) { big = true; return 0xFFFEu; }
             return uint16_t(w);
         };
-        for (int idx = tid; idx < nl * TILE * TILE; idx += NT) {
-            const int l = idx >> 10, r = (idx >> 5) & 31, c = idx & 31;
-            const float cf = S.cf[(size_t(l) * hpad + y0 + r) * pitch + x0 + c];
-            if (cf < 1e30f && !(__fmul_rn(__fmul_rn(cf, S.maxfac[l]), 16.0f) < WLIM32)) wide = true;
-            const uint32_t wx = qweight<uint32_t>(cf, S.fac[l][0]), wy = qweight<uint32_t>(cf, S.fac[l][2]);
-            const uint32_t wd = qweight<uint32_t>(cf, S.fac[l][4]);
-            const int o = l * WLS + r * CSTR + c;
-            wS[o] = w16(wx);
-            if (S.K == 3) wS[nl * WLS + o] = w16(wy);
-            wS[(S.K - 1) * nl * WLS + o] = w16(wd);
-            if (cf < 1e30f) {
-                const uint32_t mw = max(max(wx < INF32 ? wx : 0u, wy < INF32 ? wy : 0u), wd < INF32 ? wd : 0u);
-                wmax = max(wmax, static_cast<unsigned long long>(mw));
+        constexpr int WCH = 4;
+        const int groups = nl * TILE * TILE / 4;   // 4 cells of one row and layer per 128-bit load
+        for (int base = tid; base < groups; base += NT * WCH) {
+            float4 q4[WCH];
+            #pragma unroll
+            for (int u = 0; u < WCH; ++u) {
+                const int g = base + u * NT;
+                if (g < groups) {
+                    const int l = g >> 8, r = (g >> 3) & 31, c0 = (g & 7) * 4;
+                    q4[u] = *reinterpret_cast<const float4*>(S.cf + (size_t(l) * hpad + y0 + r) * pitch + x0 + c0);
+                }
+            }
+            #pragma unroll
+            for (int u = 0; u < WCH; ++u) {
+                const int g = base + u * NT;
+                if (g >= groups) break;
+                const int l = g >> 8, r = (g >> 3) & 31, c0 = (g & 7) * 4;
+                const float cv[4] = {q4[u].x, q4[u].y, q4[u].z, q4[u].w};
+                #pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const float cf = cv[e];
+                    if (cf < 1e30f && !(__fmul_rn(__fmul_rn(cf, S.maxfac[l]), 16.0f) < WLIM32)) wide = true;
+                    const uint32_t wx = qweight<uint32_t>(cf, S.fac[l][0]), wy = qweight<uint32_t>(cf, S.fac[l][2]);
+                    const uint32_t wd = qweight<uint32_t>(cf, S.fac[l][4]);
+                    const int o = l * WLS + r * CSTR + c0 + e;
+                    wS[o] = w16(wx);
+                    if (S.K == 3) wS[nl * WLS + o] = w16(wy);
+                    wS[(S.K - 1) * nl * WLS + o] = w16(wd);
+                    if (cf < 1e30f) {
+                        const uint32_t mw = max(max(wx < INF32 ? wx : 0u, wy < INF32 ? wy : 0u), wd < INF32 ? wd : 0u);
+                        wmax = max(wmax, static_cast<unsigned long long>(mw));
+                    }
+                }
             }
         }
         fallback = __syncthreads_or(big);
