@@ -748,9 +748,18 @@ __device__ void visit_tile(const SolveArgs& a, int s, int tile, int round, unsig
     const unsigned long long ub = min(ub_now, sh.tmin);
     if (sh.any) {
         DT* distw = reinterpret_cast<DT*>(S.dist);
-        for (int idx = tid; idx < nl * TILE * TILE; idx += NT) {
-            const int l = idx >> 10, r = (idx >> 5) & 31, c = idx & 31;
-            distw[(size_t(l) * hpad + y0 + r) * pitch + x0 + c] = dS[l * LS + (r + 1) * DSTR + c + 1];
+        if constexpr (sizeof(DT) == 4) {   // 16-byte stores: 4 cells of a row per store
+            for (int g = tid; g < nl * TILE * TILE / 4; g += NT) {
+                const int l = g >> 8, r = (g >> 3) & 31, c0 = (g & 7) * 4;
+                const DT* src = dS + l * LS + (r + 1) * DSTR + c0 + 1;
+                *reinterpret_cast<uint4*>(distw + (size_t(l) * hpad + y0 + r) * pitch + x0 + c0) =
+                    make_uint4(src[0], src[1], src[2], src[3]);
+            }
+        } else {
+            for (int idx = tid; idx < nl * TILE * TILE; idx += NT) {
+                const int l = idx >> 10, r = (idx >> 5) & 31, c = idx & 31;
+                distw[(size_t(l) * hpad + y0 + r) * pitch + x0 + c] = dS[l * LS + (r + 1) * DSTR + c + 1];
+            }
         }
         // an edge cell that improved (to at most the bound) below an adjacent neighbour cell's staged value:
         // that neighbour looks again. bits: 0 L, 1 R, 2 T, 3 B, 4 TL, 5 TR, 6 BL, 7 BR
