@@ -34,7 +34,7 @@ namespace pcbg {
 
 namespace {
 
-constexpr int NT = 192;                 // threads per tile block: 6 warps, one per line family and direction pair
+constexpr int NT = 384;                 // threads per tile block: 12 warps, one per line and direction
 constexpr int HS = TILE + 2;            // tile side with halo
 constexpr int DSTR = TILE + 3;          // shared row stride of distances (odd: conflict-free row, column, diagonal)
 constexpr int CSTR = TILE + 1;          // shared row stride of per-state and per-cell arrays
@@ -331,19 +331,17 @@ __device__ __forceinline__ void jstep(uint32_t* dS, const uint16_t* wP, const ui
 // Returns the positions k at which any layer's cost went down.
 template <int NL>
 __device__ __forceinline__ uint32_t walk_line(uint32_t* dS, const uint16_t* wP, const uint32_t* vS, const uint32_t* vokS,
-                                              int d0, int ds, int w0, int ws, int len, int pf, int pb) {
+                                              int d0, int ds, int w0, int ws, int len, int pf, int pb, int dir) {
+    // one direction per walker: a shortest path never turns back along a line, so the forward and the backward
+    // walks of a line are independent and run on two threads at once
     uint32_t moved = 0;
     int ch;
     uint32_t prev[NL];
+    const int start = dir ? pb : pf;
     #pragma unroll
-    for (int l = 0; l < NL; ++l) prev[l] = dS[l * LS + pf];
-    for (int k = 0; k < len; ++k) {
-        jstep<NL>(dS, wP, vS, vokS, d0 + k * ds, w0 + k * ws, prev, ch);
-        moved |= uint32_t(ch) << k;
-    }
-    #pragma unroll
-    for (int l = 0; l < NL; ++l) prev[l] = dS[l * LS + pb];
-    for (int k = len - 1; k >= 0; --k) {
+    for (int l = 0; l < NL; ++l) prev[l] = dS[l * LS + start];
+    const int k0 = dir ? len - 1 : 0, step = dir ? -1 : 1;
+    for (int t = 0, k = k0; t < len; ++t, k += step) {
         jstep<NL>(dS, wP, vS, vokS, d0 + k * ds, w0 + k * ws, prev, ch);
         moved |= uint32_t(ch) << k;
     }
@@ -368,7 +366,7 @@ constexpr int NLINES = 190;
 // Walk line `id`, then add to `mark` every line through a cell whose cost went down (its own included).
 template <int NL>
 __device__ __forceinline__ bool walk_id(const SDev& S, uint32_t* dS, const uint16_t* wS, const uint32_t* vS,
-                                        const uint32_t* vokS, int id, uint32_t (&mark)[6]) {
+                                        const uint32_t* vokS, int id, int dir, uint32_t (&mark)[6]) {
     int plane, d0, ds, w0, ws, len, pf, pb;
     int fam, a0 = 0, b0 = 0;
     if (id < 32) {
@@ -396,7 +394,7 @@ __device__ __forceinline__ bool walk_id(const SDev& S, uint32_t* dS, const uint1
         d0 = (lo + 1) * DSTR + (s - lo) + 1; ds = DSTR - 1; w0 = lo * CSTR + (s - lo); ws = CSTR - 1;
         pf = lo * DSTR + (s - lo + 2); pb = (s - lo + 2) * DSTR + lo;
     }
-    const uint32_t M = walk_line<NL>(dS, wS + plane * S.nl * WLS, vS, vokS, d0, ds, w0, ws, len, pf, pb);
+    const uint32_t M = walk_line<NL>(dS, wS + plane * S.nl * WLS, vS, vokS, d0, ds, w0, ws, len, pf, pb, dir);
     if (!M) return false;
     uint64_t d1 = 0, d2 = 0;
     if (fam == 0) {            // row r, cell (r, k): column k, diagonal k - r, anti-diagonal r + k
@@ -449,12 +447,14 @@ __device__ int relax_joint(const SDev& S, uint32_t* dS, const uint16_t* wS, cons
         if (tid < 6) dirty[cur ^ 1][tid] = 0;
         __syncthreads();
         // compact the dirty lines into list[0..total)
+        // walk units: line u forward (u < NLINES) and line u - NLINES backward
         bool d = false;
-        if (tid < NLINES) {
+        if (tid < 2 * NLINES) {
+            const int ln = tid < NLINES ? tid : tid - NLINES;
             int w, b;
-            if (tid < 64) { w = tid >> 5; b = tid & 31; }
-            else if (tid < 127) { w = 2 + ((tid - 64) >> 5); b = (tid - 64) & 31; }
-            else { w = 4 + ((tid - 127) >> 5); b = (tid - 127) & 31; }
+            if (ln < 64) { w = ln >> 5; b = ln & 31; }
+            else if (ln < 127) { w = 2 + ((ln - 64) >> 5); b = (ln - 64) & 31; }
+            else { w = 4 + ((ln - 127) >> 5); b = (ln - 127) & 31; }
             d = (dirty[cur][w] >> b) & 1u;
         }
         const unsigned bal = __ballot_sync(0xFFFFFFFFu, d);
@@ -471,7 +471,10 @@ __device__ int relax_joint(const SDev& S, uint32_t* dS, const uint16_t* wS, cons
         __syncthreads();
         uint32_t mark[6] = {0, 0, 0, 0, 0, 0};
         bool changed = false;
-        if (tid < total) changed = walk_id<NL>(S, dS, wS, vS, vokS, list[tid], mark);
+        if (tid < total) {
+            const int u = list[tid];
+            changed = walk_id<NL>(S, dS, wS, vS, vokS, u < NLINES ? u : u - NLINES, u < NLINES ? 0 : 1, mark);
+        }
         if (warp * 32 < total) {   // warps that walked: OR their marks into the next set
             #pragma unroll
             for (int w = 0; w < 6; ++w) {
@@ -815,7 +818,7 @@ __device__ void visit_tile(const SolveArgs& a, int s, int tile, int round, unsig
 }
 
 template <typename DT>
-__global__ void __launch_bounds__(NT) relax_kernel(SolveArgs a) {
+__global__ void __launch_bounds__(NT, 2) relax_kernel(SolveArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ unsigned int sh_item_hi, sh_item_lo, sh_stop;
     const unsigned int nblocks = gridDim.x;
