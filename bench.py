@@ -41,9 +41,9 @@ WORKLOAD = ("batched-search microbenchmark: 4096 seeded single-source single-tar
 BYTES_PER_LAYER_VISIT = 32 * 32 * 13     # per staged layer of a tile: cf 4 + flags 1 + distance read 4 + write 4
 BYTES_PER_TILE_VISIT = 32 * 32 * 4       # per tile: via cost of each cell
 # DRAM bytes moved per algorithmic byte by relax_kernel, from one ncu capture of the 64-search case
-# (dram__bytes_read.sum + dram__bytes_write.sum = 12.83 GB against 13.46 GB algorithmic). A full wave is too large to
+# (dram__bytes_read.sum + dram__bytes_write.sum = 11.56 GB against 12.37 GB algorithmic). A full wave is too large to
 # capture; its traffic grows with the tile visits, so the bench scales this ratio by the launch's algorithmic bytes.
-NCU_TRAFFIC_PER_ALG_BYTE = 0.953
+NCU_TRAFFIC_PER_ALG_BYTE = 0.935
 
 
 def peaks():
