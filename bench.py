@@ -372,19 +372,47 @@ def main():
     # ---- end to end: host (pinned) inputs -> device, solve, reported fields -> host, every step
     e2e = None
     if not args.no_e2e:
-        ew = dev_waves[:max(1, min(args.e2e_waves, len(dev_waves)))]
-        host_in, outs_d, outs_h, e_arrays = [], [], [], []
-        for w in ew:
-            hi = [(s["cf"].cpu().pin_memory(), s["fl"].cpu().pin_memory(), s["vcf"].cpu().pin_memory()) for s in w]
-            od = [torch.empty(s["rw"] * s["rh"] * s["nl"], dtype=torch.float32, device="cuda") for s in w]
-            oh = [torch.empty(s["rw"] * s["rh"] * s["nl"], dtype=torch.float32).pin_memory() for s in w]
-            host_in.append(hi)
-            outs_d.append(od)
-            outs_h.append(oh)
-            e_arrays.append(search_array(w, od))
-        h2d = [sum(x.numel() * x.element_size() for trip in hi for x in trip) for hi in host_in]
-        d2h = [sum(x.numel() * 4 for x in oh) for oh in outs_h]
-        e_states = [sum(s["rw"] * s["rh"] * s["nl"] for s in w) for w in ew]
+        ew_src = dev_waves[:max(1, min(args.e2e_waves, len(dev_waves)))]
+        # A caller that keeps a wave's inputs in one pinned blob and its fields in another moves each with one copy:
+        # every search's cf / flags / vcf (and its field) is a 256-byte-aligned slice of the wave's blob.
+        ew, in_d, in_h, out_d, out_h, e_arrays = [], [], [], [], [], []
+        for w in ew_src:
+            offs, off = [], 0
+            for sr in w:
+                n = sr["cf"].numel()
+                o_cf = off
+                o_fl = o_cf + -(-n * 4 // 256) * 256
+                o_vc = o_fl + -(-n // 256) * 256
+                off = o_vc + -(-sr["vcf"].numel() * 4 // 256) * 256
+                offs.append((o_cf, o_fl, o_vc))
+            blob = torch.empty(off, dtype=torch.uint8, device="cuda")
+            views = []
+            for sr, (o_cf, o_fl, o_vc) in zip(w, offs):
+                n, nv = sr["cf"].numel(), sr["vcf"].numel()
+                v = dict(sr)
+                v["cf"] = blob[o_cf:o_cf + 4 * n].view(torch.float32)
+                v["fl"] = blob[o_fl:o_fl + n]
+                v["vcf"] = blob[o_vc:o_vc + 4 * nv].view(torch.float32)
+                v["cf"].copy_(sr["cf"])
+                v["fl"].copy_(sr["fl"])
+                v["vcf"].copy_(sr["vcf"])
+                views.append(v)
+            tot = sum(sr["rw"] * sr["rh"] * sr["nl"] for sr in w)
+            od = torch.empty(tot, dtype=torch.float32, device="cuda")
+            outs, o = [], 0
+            for sr in w:
+                m = sr["rw"] * sr["rh"] * sr["nl"]
+                outs.append(od[o:o + m])
+                o += m
+            ew.append(views)
+            in_d.append(blob)
+            in_h.append(blob.cpu().pin_memory())
+            out_d.append(od)
+            out_h.append(torch.empty(tot, dtype=torch.float32).pin_memory())
+            e_arrays.append(search_array(views, outs))
+        h2d = [x.numel() for x in in_h]
+        d2h = [x.numel() * 4 for x in out_h]
+        e_states = [sum(sr["rw"] * sr["rh"] * sr["nl"] for sr in w) for w in ew]
 
         # Steps are pipelined the way a caller with two wave buffers would run them: the inputs of step k+1 go up
         # on one copy stream and the fields of step k come down on another while step k+1's launch runs. Every
@@ -396,10 +424,7 @@ def main():
         def e2e_h2d(k):
             i = k % len(ew)
             with torch.cuda.stream(cs_in):
-                for s, (hc, hf, hv) in zip(ew[i], host_in[i]):
-                    s["cf"].copy_(hc, non_blocking=True)
-                    s["fl"].copy_(hf, non_blocking=True)
-                    s["vcf"].copy_(hv, non_blocking=True)
+                in_d[i].copy_(in_h[i], non_blocking=True)
                 ev_in[i].record(cs_in)
 
         def e2e_solve(k):
@@ -411,8 +436,7 @@ def main():
                 raise RuntimeError("pcbg_solve_batch failed: " + _lib.last_error())
             cs_out.wait_stream(stream)
             with torch.cuda.stream(cs_out):
-                for od, oh in zip(outs_d[i], outs_h[i]):
-                    oh.copy_(od, non_blocking=True)
+                out_h[i].copy_(out_d[i], non_blocking=True)
                 ev_out[i].record(cs_out)
             return e_states[i], h2d[i], d2h[i]
 
@@ -444,8 +468,9 @@ def main():
         et, etot = replicas.max_time_sum_work(f0.elapsed_time(f1), es, "cuda", ws)
         e2e = {"value": round(9.0 * etot / (et / 1e3) / 1e9, 4), "unit": UNIT,
                "h2d_bytes_per_step": int(eb_in // args.steps), "d2h_bytes_per_step": int(eb_out // args.steps),
-               "waves": len(ew), "api": "pcbg_solve_batch from pinned host buffers, reported fields read back; "
-                                              "copies of neighbouring steps overlap the launch on two copy streams"}
+               "waves": len(ew), "api": "pcbg_solve_batch from pinned host buffers, reported fields read back; one copy each "
+                                              "way per wave, overlapping the neighbouring steps' launches on two "
+                                              "copy streams"}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
