@@ -1116,8 +1116,10 @@ int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream
     a.visits = static_cast<unsigned long long*>(A.visits.p);
     a.max_rounds = 1 << 20;
     seed_kernel<DT><<<m, 128, 0, stream>>>(a, d_sip, d_sdp, d_ns);
-    const int blocks = occupancy_blocks<DT>(smem);
-    if (blocks <= 0) { t_err = "relax kernel cannot be resident"; return -1; }
+    const int resident = occupancy_blocks<DT>(smem);
+    if (resident <= 0) { t_err = "relax kernel cannot be resident"; return -1; }
+    // a round visits each queued tile once: more blocks than tiles would only wait at the grid barriers
+    const int blocks = int(std::min<size_t>(size_t(resident), std::max<size_t>(tiles, 1)));
     void* args[] = {&a};
     if (!g_ev0) { cudaEventCreate(&g_ev0); cudaEventCreate(&g_ev1); }
     cudaEventRecord(g_ev0, stream);
