@@ -8,10 +8,11 @@
 //   * the window is cut into 32 x 32-cell tiles holding every layer; a tile visit stages the tile's distances
 //     (with a one-cell halo from its neighbours), integer move weights, via weights and via/target masks in shared
 //     memory and relaxes them to a local fixed point;
-//   * the local relaxation scans lines (rows, columns, both diagonals, each way) with all layers of a line in one
-//     thread, mixing vias at every cell of the line, so a path that changes layers along a straight run settles in
-//     one pass; the four line families run at once on separate warps, with shared-memory atomicMin updates so that
-//     every stored value only decreases;
+//   * the local relaxation scans lines (rows, columns, both diagonals) with all layers of a line in one thread,
+//     mixing vias at every cell of the line, so a path that changes layers along a straight run settles in one
+//     pass; the forward and backward walks of a line run on two threads at once, and only lines through cells that
+//     went down are walked again; all walks of an iteration run concurrently, with shared-memory atomicMin updates
+//     so that every stored value only decreases;
 //   * a tile whose edge cell improved below the staged value of an adjacent cell of a neighbour (and not above the
 //     best target found so far) queues that neighbour for the next round;
 //   * one persistent cooperative launch runs all rounds of all searches of a batch, with a bounded software grid
@@ -427,9 +428,11 @@ __device__ __forceinline__ bool walk_id(const SDev& S, uint32_t* dS, const uint1
     return true;
 }
 
-// Relax a tile to its local fixed point. Every line starts dirty; each iteration walks only the dirty lines, packed
-// onto the fewest warps, and marks the lines through the cells that went down. The visit ends after an iteration
-// with no dirty line, i.e. after a pass in which no line changed anything.
+// Relax a tile to its local fixed point. The lines whose end cells read a changed halo side start dirty (every
+// line after a start was written or a visit stopped early). Each iteration walks every dirty line both ways, one
+// walk unit per thread, packed onto the fewest warps, and marks the lines through the cells that went down, the
+// walked line included (its other direction may have passed those cells before they went down). The visit ends
+// after an iteration with no dirty line, i.e. after a pass in which no line changed anything.
 template <int NL>
 __device__ int relax_joint(const SDev& S, uint32_t* dS, const uint16_t* wS, const uint32_t* vS, const uint32_t* vokS,
                            VisitShared& sh, bool& requeue) {
