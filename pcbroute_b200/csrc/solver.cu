@@ -1014,6 +1014,23 @@ thread_local std::string t_err;
 thread_local BatchStats t_stats;
 cudaEvent_t g_ev0 = nullptr, g_ev1 = nullptr;
 
+// pinned host staging of a batch's descriptors and results (batches are serialised by g_mu)
+struct HostStage {
+    unsigned char* p = nullptr;
+    size_t cap = 0;
+} g_hstage;
+
+bool host_stage(size_t n) {
+    if (g_hstage.cap >= n) return true;
+    if (g_hstage.p) cudaFreeHost(g_hstage.p);
+    g_hstage.p = nullptr;
+    g_hstage.cap = 0;
+    const size_t c = n + n / 2 + 4096;
+    if (cudaHostAlloc(reinterpret_cast<void**>(&g_hstage.p), c, cudaHostAllocDefault) != cudaSuccess) return false;
+    g_hstage.cap = c;
+    return true;
+}
+
 template <typename DT> int occupancy_blocks(size_t smem) {
     if (cudaFuncSetAttribute(relax_kernel<DT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess) return -1;
     int per_sm = 0;
@@ -1088,21 +1105,28 @@ int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream
         sd[k].stamp = static_cast<uint32_t*>(A.stamp.p) + toff[k];
         sd[k].sides = static_cast<uint32_t*>(A.stamp.p) + tiles + toff[k];
     }
-    std::vector<const uint32_t*> sip(m);
-    std::vector<const uint64_t*> sdp(m);
-    std::vector<int> nsv(m);
-    for (int k = 0; k < m; ++k) { sip[k] = items[idx[k]].start_idx; sdp[k] = items[idx[k]].start_d; nsv[k] = items[idx[k]].n_starts; }
+    // the batch's descriptors, initial stats and start lists go up from pinned staging (asynchronous copies; a copy
+    // from pageable memory would go through the driver's bounce buffer one call at a time)
+    const size_t h_sd = 0, h_st = round_up(sizeof(SDev) * m, 16), h_sp = h_st + round_up(sizeof(SStat) * m, 16);
+    const size_t h_res = h_sp + round_up(size_t(m) * 20, 16), h_ctl = h_res + round_up(sizeof(SStat) * m, 16);
+    const size_t h_vis = h_ctl + 64, h_end = h_vis + 32;
+    if (!host_stage(h_end)) { t_err = "pinned allocation failed"; return -1; }
+    unsigned char* hs = g_hstage.p;
+    memcpy(hs + h_sd, sd.data(), sizeof(SDev) * m);
+    SStat* st0 = reinterpret_cast<SStat*>(hs + h_st);
+    for (int k = 0; k < m; ++k) {
+        st0[k].ub = ~0ull; st0[k].maxw = 0; st0[k].best = ~0ull; st0[k].maxd = 0; st0[k].need_wide = 0; st0[k].pad = 0;
+        reinterpret_cast<const uint32_t**>(hs + h_sp)[k] = items[idx[k]].start_idx;
+        reinterpret_cast<const uint64_t**>(hs + h_sp + size_t(m) * 8)[k] = items[idx[k]].start_d;
+        reinterpret_cast<int*>(hs + h_sp + size_t(m) * 16)[k] = items[idx[k]].n_starts;
+    }
     unsigned char* sp = static_cast<unsigned char*>(A.sptr.p);
     const uint32_t* const* d_sip = reinterpret_cast<const uint32_t* const*>(sp);
     const uint64_t* const* d_sdp = reinterpret_cast<const uint64_t* const*>(sp + size_t(m) * 8);
     const int* d_ns = reinterpret_cast<const int*>(sp + size_t(m) * 16);
-    std::vector<SStat> st0(m);
-    for (auto& x : st0) { x.ub = ~0ull; x.maxw = 0; x.best = ~0ull; x.maxd = 0; x.need_wide = 0; x.pad = 0; }
-    cudaMemcpyAsync(A.sdev.p, sd.data(), sizeof(SDev) * m, cudaMemcpyHostToDevice, stream);
-    cudaMemcpyAsync(A.sstat.p, st0.data(), sizeof(SStat) * m, cudaMemcpyHostToDevice, stream);
-    cudaMemcpyAsync(sp, sip.data(), size_t(m) * 8, cudaMemcpyHostToDevice, stream);
-    cudaMemcpyAsync(sp + size_t(m) * 8, sdp.data(), size_t(m) * 8, cudaMemcpyHostToDevice, stream);
-    cudaMemcpyAsync(sp + size_t(m) * 16, nsv.data(), size_t(m) * 4, cudaMemcpyHostToDevice, stream);
+    cudaMemcpyAsync(A.sdev.p, hs + h_sd, sizeof(SDev) * m, cudaMemcpyHostToDevice, stream);
+    cudaMemcpyAsync(A.sstat.p, hs + h_st, sizeof(SStat) * m, cudaMemcpyHostToDevice, stream);
+    cudaMemcpyAsync(sp, hs + h_sp, size_t(m) * 20, cudaMemcpyHostToDevice, stream);
     cudaMemsetAsync(A.dist.p, 0x7F, dbytes, stream);
     cudaMemsetAsync(A.stamp.p, 0, tiles * 8 + 8, stream);
     cudaMemsetAsync(A.ctl.p, 0, C_N * 4, stream);
@@ -1135,12 +1159,12 @@ int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream
         walkback_kernel<DT><<<m, 32, 0, stream>>>(a.S, a.st, d_sip, d_sdp, d_ns);
         bs.launches += 1;
     }
-    std::vector<SStat> st(m);
-    unsigned int ctl[C_N];
-    unsigned long long visits[3] = {0, 0, 0};
-    cudaMemcpyAsync(st.data(), A.sstat.p, sizeof(SStat) * m, cudaMemcpyDeviceToHost, stream);
-    cudaMemcpyAsync(ctl, A.ctl.p, sizeof(ctl), cudaMemcpyDeviceToHost, stream);
-    cudaMemcpyAsync(visits, A.visits.p, 24, cudaMemcpyDeviceToHost, stream);
+    const SStat* st = reinterpret_cast<const SStat*>(hs + h_res);
+    const unsigned int* ctl = reinterpret_cast<const unsigned int*>(hs + h_ctl);
+    const unsigned long long* visits = reinterpret_cast<const unsigned long long*>(hs + h_vis);
+    cudaMemcpyAsync(hs + h_res, A.sstat.p, sizeof(SStat) * m, cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(hs + h_ctl, A.ctl.p, C_N * 4, cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(hs + h_vis, A.visits.p, 24, cudaMemcpyDeviceToHost, stream);
     e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) { t_err = std::string("batch solve: ") + cudaGetErrorString(e); return -1; }
     if (ctl[C_ERR]) {
