@@ -108,6 +108,8 @@ struct pcbg_spec {
     pcbg::DBuf<uint64_t> sd;
     pcbg::DBuf<int> plen;
     pcbg::DBuf<pcbg::WinDesc> wd;
+    unsigned char* hpin = nullptr;               // pinned staging of a batch's uploads and of its paths
+    size_t hpin_cap = 0;
     pcbg_spec_scheduler sched = nullptr;        // learned batch composition (PCBG_SPEC_LEARNED)
     void* sched_user = nullptr;
     pcbg_spec_observer observer = nullptr;      // called once per speculative search (conflict logs)
@@ -118,6 +120,17 @@ namespace pcbg {
 namespace {
 
 int bw_of(const pcbg_spec* S) { return (S->P.nx + BS - 1) / BS; }
+
+bool pinned(pcbg_spec* S, size_t n) {
+    if (S->hpin_cap >= n) return true;
+    if (S->hpin) cudaFreeHost(S->hpin);
+    S->hpin = nullptr;
+    S->hpin_cap = 0;
+    const size_t c = n + n / 2 + 4096;
+    if (cudaHostAlloc(reinterpret_cast<void**>(&S->hpin), c, cudaHostAllocDefault) != cudaSuccess) return false;
+    S->hpin_cap = c;
+    return true;
+}
 
 // Search nets B (indices) in one batch; paths come back as board states, target first (empty: no path).
 int run_searches(pcbg_spec* S, const std::vector<int>& B, std::vector<std::vector<uint32_t>>& out, double& ms,
@@ -143,18 +156,24 @@ int run_searches(pcbg_spec* S, const std::vector<int>& B, std::vector<std::vecto
         set_error("device allocation failed");
         return -1;
     }
-    std::vector<uint32_t> si(n);
-    std::vector<uint64_t> sd(n, 0);
+    // uploads from pinned staging: window descriptors, then start states, then start costs (all zero)
+    const size_t o_si = round_up(n * sizeof(WinDesc), 16), o_sd = o_si + round_up(size_t(n) * 4, 16);
+    const size_t o_pl = o_sd + size_t(n) * 8;
+    if (!pinned(S, o_pl + size_t(n) * 4)) { set_error("pinned allocation failed"); return -1; }
+    memcpy(S->hpin, wd.data(), n * sizeof(WinDesc));
+    uint32_t* si = reinterpret_cast<uint32_t*>(S->hpin + o_si);
+    uint64_t* sd = reinterpret_cast<uint64_t*>(S->hpin + o_sd);
     const size_t board = size_t(S->P.nx) * S->P.ny;
     for (int k = 0; k < n; ++k) {
         const pcbg_net& N = S->nets[B[k]];
         const int sl = int(N.src / board), sc = int(N.src % board), sy = sc / S->P.nx, sx = sc % S->P.nx;
         si[k] = uint32_t((size_t(sl) * wd[k].rh + (sy - N.y0)) * wd[k].rw + (sx - N.x0));
+        sd[k] = 0;
     }
     cudaStream_t st = S->stream;
-    cudaMemcpyAsync(S->wd.p, wd.data(), n * sizeof(WinDesc), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(S->si.p, si.data(), n * 4, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(S->sd.p, sd.data(), n * 8, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(S->wd.p, S->hpin, n * sizeof(WinDesc), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(S->si.p, si, n * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(S->sd.p, sd, n * 8, cudaMemcpyHostToDevice, st);
     spec_resolve_kernel<<<dim3(64, n), 256, 0, st>>>(S->P, S->wd.p, nl, S->via_cost, S->cf.p, S->fl.p, S->vcf.p);
     if (cudaGetLastError() != cudaSuccess) {   // the batch launch follows on the same stream
         set_error("window resolve failed");
@@ -179,22 +198,30 @@ int run_searches(pcbg_spec* S, const std::vector<int>& B, std::vector<std::vecto
     }
     if (solve_batch(items.data(), n, st) != 0) return -1;
     relax_ms += last_stats().kernel_ms;
+    // path lengths, then every path, into pinned staging
     std::vector<int> plen(n);
-    cudaMemcpyAsync(plen.data(), S->plen.p, n * 4, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(S->hpin + o_pl, S->plen.p, n * 4, cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) { set_error("path read failed"); return -1; }
-    out.assign(n, {});
-    std::vector<std::vector<uint32_t>> rect(n);
+    memcpy(plen.data(), S->hpin + o_pl, n * 4);
+    size_t total = 0;
+    std::vector<size_t> hoff(n);
     for (int k = 0; k < n; ++k) {
         if (plen[k] < 0) { set_error("walk-back failed"); return -1; }
-        rect[k].resize(plen[k]);
-        if (plen[k]) cudaMemcpyAsync(rect[k].data(), S->pbuf.p + poffs[k], size_t(plen[k]) * 4, cudaMemcpyDeviceToHost, st);
+        hoff[k] = total;
+        total += size_t(plen[k]);
     }
+    if (!pinned(S, total * 4 + 16)) { set_error("pinned allocation failed"); return -1; }
+    uint32_t* hp = reinterpret_cast<uint32_t*>(S->hpin);
+    for (int k = 0; k < n; ++k)
+        if (plen[k]) cudaMemcpyAsync(hp + hoff[k], S->pbuf.p + poffs[k], size_t(plen[k]) * 4, cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) { set_error("path read failed"); return -1; }
+    out.assign(n, {});
     for (int k = 0; k < n; ++k) {
         const WinDesc& W = wd[k];
         const size_t RN = size_t(W.rw) * W.rh;
-        out[k].reserve(rect[k].size());
-        for (uint32_t r : rect[k]) {
+        out[k].reserve(size_t(plen[k]));
+        for (int q = 0; q < plen[k]; ++q) {
+            const uint32_t r = hp[hoff[k] + q];
             const size_t l = r / RN, c = r % RN;
             const int j = int(c / W.rw), i = int(c % W.rw);
             out[k].push_back(uint32_t(l * board + size_t(W.y0 + j) * S->P.nx + (W.x0 + i)));
@@ -306,6 +333,7 @@ extern "C" void pcbg_spec_destroy(pcbg_spec* S) {
     cudaStreamSynchronize(S->stream);
     S->cf.release(); S->vcf.release(); S->fl.release(); S->si.release(); S->pbuf.release();
     S->sd.release(); S->plen.release(); S->wd.release();
+    if (S->hpin) cudaFreeHost(S->hpin);
     cudaStreamDestroy(S->stream);
     delete S;
 }
