@@ -154,8 +154,8 @@ def learned_batching():
     """The speculative negotiation rounds on seeded 320 x 256 x 6 boards of 160 nets: the conflict predictor trained
     on the logs of plain rounds over 4 boards, then 3 rip-up-and-reroute iterations on 2 held-out boards with one
     search per launch (sequential), the plain batching (lookahead 16) and the learned batching. Host time of the
-    rounds (searches, walk-backs, commits), the wasted-search fraction, and whether all three committed the same
-    paths."""
+    rounds (searches, walk-backs, commits; the faster of 2 runs per board and iteration), the wasted-search
+    fraction, and whether all three committed the same paths."""
     from pcbroute_b200 import sched
     kw = dict(nx=320, ny=256, nl=6, nnets=160, margin=12, span=(16, 128))
     r = sched.ab_report(range(100, 104), range(900, 902), kw, iters=3, width=16, epochs=12)

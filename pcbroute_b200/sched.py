@@ -125,11 +125,15 @@ def run(b: dict, iters: int, width: int, sch: Scheduler | None = None, threshold
 
 
 def ab_report(train_seeds, test_seeds, board_kw: dict, iters: int = 3, width: int = 16, epochs: int = 12,
-              threshold: float = 0.5, seed: int = 21) -> dict:
+              threshold: float = 0.5, seed: int = 21, repeat: int = 2) -> dict:
     """Train on the conflict logs of plain rounds over `train_seeds` boards, then negotiate the `test_seeds` boards
     sequentially (one search per launch), with the plain batching and with the learned one. Returns the totals per
     method (searches, wasted searches, launches, host and device milliseconds) and whether all three committed the
-    same paths."""
+    same paths.
+
+    Each method negotiates each board `repeat` times. The searches, launches and paths are deterministic, so every
+    repeat gives the same counts; the milliseconds of an iteration are the lowest over the repeats, which keeps a
+    stall of the host thread in one repeat out of the totals."""
     import time
     train = [spec.spec_board(s, **board_kw) for s in train_seeds]
     test = [spec.spec_board(s, **board_kw) for s in test_seeds]
@@ -149,23 +153,33 @@ def ab_report(train_seeds, test_seeds, board_kw: dict, iters: int = 3, width: in
                          ("learned", spec.LEARNED, sch)):
         tot = dict(searches=0, wasted=0, batches=0, total_ms=0.0, search_ms=0.0, relax_ms=0.0)
         for b in test:
-            r = spec.Round(b)
-            try:
-                if s is not None:
-                    s.attach(r, threshold)
-                for it in range(iters):
-                    st = r.iterate(spec.pres_of(it), pol, width)
-                    for k in tot:
-                        tot[k] += st[k]
-                    if it + 1 < iters:
-                        r.add_history(1.0)
-                paths = r.paths()
-            finally:
-                r.close()
-            if name == "sequential":
-                ref[b["seed"]] = paths
-            else:
-                same &= all(np.array_equal(a, c) for a, c in zip(ref[b["seed"]], paths))
+            best = [None] * iters
+            for rep in range(max(1, repeat)):
+                r = spec.Round(b)
+                try:
+                    if s is not None:
+                        s.attach(r, threshold)
+                    for it in range(iters):
+                        st = r.iterate(spec.pres_of(it), pol, width)
+                        if best[it] is None:
+                            best[it] = dict(st)
+                        else:
+                            for k in ("searches", "wasted", "batches"):
+                                same &= best[it][k] == st[k]
+                            for k in ("total_ms", "search_ms", "relax_ms"):
+                                best[it][k] = min(best[it][k], st[k])
+                        if it + 1 < iters:
+                            r.add_history(1.0)
+                    paths = r.paths()
+                finally:
+                    r.close()
+                if name == "sequential" and rep == 0:
+                    ref[b["seed"]] = paths
+                else:
+                    same &= all(np.array_equal(a, c) for a, c in zip(ref[b["seed"]], paths))
+            for st in best:
+                for k in tot:
+                    tot[k] += st[k]
         tot["wasted_fraction"] = round(tot["wasted"] / max(1, tot["searches"]), 4)
         for k in ("total_ms", "search_ms", "relax_ms"):
             tot[k] = round(tot[k], 1)
@@ -189,9 +203,11 @@ def main() -> None:
     ap.add_argument("--width", type=int, default=16)
     ap.add_argument("--epochs", type=int, default=12)
     ap.add_argument("--threshold", type=float, default=0.5)
+    ap.add_argument("--repeat", type=int, default=2, help="negotiations per board and method; the fastest counts")
     a = ap.parse_args()
     kw = dict(nx=a.nx, ny=a.ny, nl=a.nl, nnets=a.nets, margin=12, span=(16, max(24, min(a.nx, a.ny) // 2)))
-    r = ab_report(range(100, 100 + a.train), range(900, 900 + a.test), kw, a.iters, a.width, a.epochs, a.threshold)
+    r = ab_report(range(100, 100 + a.train), range(900, 900 + a.test), kw, a.iters, a.width, a.epochs, a.threshold,
+                  repeat=a.repeat)
     print(json.dumps(r))
 
 
