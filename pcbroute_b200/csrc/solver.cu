@@ -320,7 +320,8 @@ __device__ __forceinline__ void jstep(uint32_t* dS, const uint16_t* wP, const ui
     for (int l = 0; l < NL; ++l) {
         c[l] = ((vm >> l) & 1u) ? min(c[l], mv) : c[l];
         any |= uint32_t(c[l] < v[l]);
-        atomicMin(dS + l * LS + dofs, c[l]);   // unconditional: no branch; a min that lowers nothing is harmless
+        atomicMin(dS + l * LS + dofs, c[l]);   // unconditional: a min that lowers nothing is harmless, and cheaper
+                                               // than an atomic predicated on c < v
         prev[l] = c[l];
     }
     ch = int(any);
@@ -428,72 +429,79 @@ __device__ __forceinline__ bool walk_id(const SDev& S, uint32_t* dS, const uint1
     return true;
 }
 
+// Position of set bit k (counted from 0) of x; x has more than k set bits.
+__device__ __forceinline__ int select_bit(uint32_t x, int k) {
+    int pos = 0, c;
+    c = __popc(x & 0xFFFFu); if (k >= c) { k -= c; x >>= 16; pos += 16; }
+    c = __popc(x & 0xFFu);   if (k >= c) { k -= c; x >>= 8;  pos += 8; }
+    c = __popc(x & 0xFu);    if (k >= c) { k -= c; x >>= 4;  pos += 4; }
+    c = __popc(x & 0x3u);    if (k >= c) { k -= c; x >>= 2;  pos += 2; }
+    return pos + (k >= int(x & 1u) ? 1 : 0);
+}
+
 // Relax a tile to its local fixed point. The lines whose end cells read a changed halo side start dirty (every
 // line after a start was written or a visit stopped early). Each iteration walks every dirty line both ways, one
 // walk unit per thread, packed onto the fewest warps, and marks the lines through the cells that went down, the
 // walked line included (its other direction may have passed those cells before they went down). The visit ends
 // after an iteration with no dirty line, i.e. after a pass in which no line changed anything.
+//
+// One block barrier per iteration. The dirty sets rotate through three buffers: an iteration reads one, ORs its
+// marks into the next, and clears the third, which the previous iteration read and the next one writes. With P
+// dirty lines, thread t < P walks the t-th dirty line forward and thread P + t walks it backward; each thread
+// finds its line by popcounts over the 6 words, so the units need no compacted list.
 template <int NL>
 __device__ int relax_joint(const SDev& S, uint32_t* dS, const uint16_t* wS, const uint32_t* vS, const uint32_t* vokS,
                            VisitShared& sh, bool& requeue) {
-    __shared__ uint32_t dirty[2][6];
-    __shared__ uint16_t list[NT];
-    __shared__ int wcount[NT / 32];
+    __shared__ uint32_t dirty[3][6];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid == 0) {
         uint32_t w[6];
         side_lines(sh.sides, w);
-        for (int k = 0; k < 6; ++k) dirty[0][k] = w[k];
+        for (int k = 0; k < 6; ++k) { dirty[0][k] = w[k]; dirty[1][k] = 0; dirty[2][k] = 0; }
     }
-    int cur = 0;
+    int cur = 0, nxt = 1, old = 2;
     for (int it = 0;; ++it) {
-        if (tid < 6) dirty[cur ^ 1][tid] = 0;
         __syncthreads();
-        // compact the dirty lines into list[0..total)
-        // walk units: line u forward (u < NLINES) and line u - NLINES backward
-        bool d = false;
-        if (tid < 2 * NLINES) {
-            const int ln = tid < NLINES ? tid : tid - NLINES;
-            int w, b;
-            if (ln < 64) { w = ln >> 5; b = ln & 31; }
-            else if (ln < 127) { w = 2 + ((ln - 64) >> 5); b = (ln - 64) & 31; }
-            else { w = 4 + ((ln - 127) >> 5); b = (ln - 127) & 31; }
-            d = (dirty[cur][w] >> b) & 1u;
-        }
-        const unsigned bal = __ballot_sync(0xFFFFFFFFu, d);
-        if (lane == 0) wcount[warp] = __popc(bal);
-        __syncthreads();
-        int off = 0, total = 0;
+        uint32_t w[6];
+        int pc[6], P = 0;
         #pragma unroll
-        for (int w = 0; w < NT / 32; ++w) {
-            off += w < warp ? wcount[w] : 0;
-            total += wcount[w];
+        for (int k = 0; k < 6; ++k) {
+            w[k] = dirty[cur][k];
+            pc[k] = __popc(w[k]);
+            P += pc[k];
         }
-        if (d) list[off + __popc(bal & ((1u << lane) - 1u))] = uint16_t(tid);
-        if (total == 0) return it;
-        __syncthreads();
+        if (P == 0) return it;
+        if (tid < 6) dirty[old][tid] = 0;
+        const int total = 2 * P;
         uint32_t mark[6] = {0, 0, 0, 0, 0, 0};
         bool changed = false;
         if (tid < total) {
-            const int u = list[tid];
-            changed = walk_id<NL>(S, dS, wS, vS, vokS, u < NLINES ? u : u - NLINES, u < NLINES ? 0 : 1, mark);
+            const int dir = tid < P ? 0 : 1;
+            int k = dir ? tid - P : tid, base = 0;
+            uint32_t x = w[0];
+            if (k >= pc[0]) { k -= pc[0]; base = 32; x = w[1];
+                if (k >= pc[1]) { k -= pc[1]; base = 64; x = w[2];
+                    if (k >= pc[2]) { k -= pc[2]; base = 96; x = w[3];
+                        if (k >= pc[3]) { k -= pc[3]; base = 127; x = w[4];
+                            if (k >= pc[4]) { k -= pc[4]; base = 159; x = w[5]; } } } } }
+            changed = walk_id<NL>(S, dS, wS, vS, vokS, base + select_bit(x, k), dir, mark);
         }
-        if (warp * 32 < total) {   // warps that walked: OR their marks into the next set
+        if (warp * 32 < total) {
             #pragma unroll
-            for (int w = 0; w < 6; ++w) {
-                const uint32_t m = __reduce_or_sync(0xFFFFFFFFu, mark[w]);
-                if (lane == 0 && m) atomicOr(&dirty[cur ^ 1][w], m);
+            for (int q = 0; q < 6; ++q) {
+                const uint32_t m = __reduce_or_sync(0xFFFFFFFFu, mark[q]);
+                if (lane == 0 && m) atomicOr(&dirty[nxt][q], m);
             }
             if (__any_sync(0xFFFFFFFFu, changed) && lane == 0) sh.any = 1;
         }
-        cur ^= 1;
         if (it + 1 >= MAX_IT) {
             __syncthreads();
             bool left = false;
-            if (tid < 6) left = dirty[cur][tid] != 0;
+            if (tid < 6) left = dirty[nxt][tid] != 0;
             if (__syncthreads_or(left)) requeue = true;
             return it + 1;
         }
+        const int t = cur; cur = nxt; nxt = old; old = t;
     }
 }
 
