@@ -828,8 +828,11 @@ __device__ void visit_tile(const SolveArgs& a, int s, int tile, int round, unsig
     __syncthreads();
 }
 
-template <typename DT>
-__global__ void __launch_bounds__(NT, 2) relax_kernel(SolveArgs a) {
+// Two builds of the kernel: MINB = 2 blocks per SM with up to 80 registers a thread, or MINB = 3 within 56
+// registers (the 32-bit build spills 80 bytes). A third resident block fills more of the time that warps wait at the
+// local-iteration barrier; relax_launch takes it wherever the visit's shared memory lets 3 blocks reside.
+template <typename DT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) relax_kernel(SolveArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ unsigned int sh_item_hi, sh_item_lo, sh_stop;
     const unsigned int nblocks = gridDim.x;
@@ -1039,14 +1042,28 @@ bool host_stage(size_t n) {
     return true;
 }
 
-template <typename DT> int occupancy_blocks(size_t smem) {
-    if (cudaFuncSetAttribute(relax_kernel<DT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess) return -1;
+template <typename DT, int MINB> int blocks_per_sm(size_t smem) {
+    if (cudaFuncSetAttribute(relax_kernel<DT, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
+        return -1;
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, relax_kernel<DT>, NT, smem) != cudaSuccess) return -1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, relax_kernel<DT, MINB>, NT, smem) != cudaSuccess) return -1;
+    return per_sm;
+}
+
+// The relax kernel build for a launch with `smem` bytes of dynamic shared memory, and how many of its blocks are
+// resident on the device at once (<= 0: none can be).
+struct RelaxLaunch {
+    void* fn;
+    int resident;
+};
+template <typename DT> RelaxLaunch relax_launch(size_t smem) {
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    return per_sm * sms;
+    const int p3 = blocks_per_sm<DT, 3>(smem);
+    if (p3 >= 3) return {reinterpret_cast<void*>(relax_kernel<DT, 3>), p3 * sms};
+    const int p2 = blocks_per_sm<DT, 2>(smem);
+    return {reinterpret_cast<void*>(relax_kernel<DT, 2>), p2 < 0 ? -1 : p2 * sms};
 }
 
 // joint mode needs one factor per move class on every layer (true of every query the router builds)
@@ -1151,14 +1168,14 @@ int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream
     a.visits = static_cast<unsigned long long*>(A.visits.p);
     a.max_rounds = 1 << 20;
     seed_kernel<DT><<<m, 128, 0, stream>>>(a, d_sip, d_sdp, d_ns);
-    const int resident = occupancy_blocks<DT>(smem);
-    if (resident <= 0) { t_err = "relax kernel cannot be resident"; return -1; }
+    const RelaxLaunch R = relax_launch<DT>(smem);
+    if (R.resident <= 0) { t_err = "relax kernel cannot be resident"; return -1; }
     // a round visits each queued tile once: more blocks than tiles would only wait at the grid barriers
-    const int blocks = int(std::min<size_t>(size_t(resident), std::max<size_t>(tiles, 1)));
+    const int blocks = int(std::min<size_t>(size_t(R.resident), std::max<size_t>(tiles, 1)));
     void* args[] = {&a};
     if (!g_ev0) { cudaEventCreate(&g_ev0); cudaEventCreate(&g_ev1); }
     cudaEventRecord(g_ev0, stream);
-    cudaError_t e = cudaLaunchCooperativeKernel(reinterpret_cast<void*>(relax_kernel<DT>), dim3(blocks), dim3(NT), args, smem, stream);
+    cudaError_t e = cudaLaunchCooperativeKernel(R.fn, dim3(blocks), dim3(NT), args, smem, stream);
     if (e != cudaSuccess) { t_err = std::string("cooperative launch: ") + cudaGetErrorString(e); return -1; }
     cudaEventRecord(g_ev1, stream);
     report_kernel<DT><<<dim3(32, m), 256, 0, stream>>>(a.S, a.st);
@@ -1364,10 +1381,11 @@ int na_run(pcbg_search* q, unsigned char* base, cudaStream_t stream) {
                                           reinterpret_cast<const uint64_t* const*>(small + NA_SPTR + 8),
                                           reinterpret_cast<const int*>(small + NA_SPTR + 16));
     const size_t smem = S.mode ? layout(q->nl, joint_wbytes(S.K), 4).total : layout(q->nl, 4, sizeof(DT)).total;
-    const int blocks = occupancy_blocks<DT>(smem);
+    const RelaxLaunch R = relax_launch<DT>(smem);
+    const int blocks = R.resident;
     if (blocks <= 0) { na_error("relax kernel cannot be resident%s"); return -1; }
     void* args[] = {&a};
-    cudaError_t e = cudaLaunchCooperativeKernel(reinterpret_cast<void*>(relax_kernel<DT>), dim3(blocks), dim3(NT), args, smem, stream);
+    cudaError_t e = cudaLaunchCooperativeKernel(R.fn, dim3(blocks), dim3(NT), args, smem, stream);
     if (e != cudaSuccess) { na_error("cooperative launch: %s", cudaGetErrorString(e)); return -1; }
     report_kernel<DT><<<dim3(32, 1), 256, 0, stream>>>(a.S, a.st);
     SStat x;
