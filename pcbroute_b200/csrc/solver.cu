@@ -830,7 +830,7 @@ __device__ void visit_tile(const SolveArgs& a, int s, int tile, int round, unsig
 
 // Two builds of the kernel: MINB = 2 blocks per SM with up to 80 registers a thread, or MINB = 3 within 56
 // registers (the 32-bit build spills 80 bytes). A third resident block fills more of the time that warps wait at the
-// local-iteration barrier; relax_launch takes it wherever the visit's shared memory lets 3 blocks reside.
+// local-iteration barrier, but each block runs slower; relax_launch takes it only for batches with many tiles.
 template <typename DT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) relax_kernel(SolveArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -1050,18 +1050,22 @@ template <typename DT, int MINB> int blocks_per_sm(size_t smem) {
     return per_sm;
 }
 
-// The relax kernel build for a launch with `smem` bytes of dynamic shared memory, and how many of its blocks are
-// resident on the device at once (<= 0: none can be).
+// The relax kernel build for a launch over `tiles` tiles with `smem` bytes of dynamic shared memory, and how many of
+// its blocks are resident on the device at once (<= 0: none can be). The 3-block build pays only when rounds queue
+// far more tiles than blocks: a batch of at least 16 tiles per resident block (a 512-search wave of the
+// microbenchmark has about 170 K tiles; one search or a speculative round a few thousand at most).
 struct RelaxLaunch {
     void* fn;
     int resident;
 };
-template <typename DT> RelaxLaunch relax_launch(size_t smem) {
+template <typename DT> RelaxLaunch relax_launch(size_t smem, size_t tiles) {
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int p3 = blocks_per_sm<DT, 3>(smem);
-    if (p3 >= 3) return {reinterpret_cast<void*>(relax_kernel<DT, 3>), p3 * sms};
+    if (tiles >= size_t(16) * 3 * sms) {
+        const int p3 = blocks_per_sm<DT, 3>(smem);
+        if (p3 >= 3) return {reinterpret_cast<void*>(relax_kernel<DT, 3>), p3 * sms};
+    }
     const int p2 = blocks_per_sm<DT, 2>(smem);
     return {reinterpret_cast<void*>(relax_kernel<DT, 2>), p2 < 0 ? -1 : p2 * sms};
 }
@@ -1168,7 +1172,7 @@ int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream
     a.visits = static_cast<unsigned long long*>(A.visits.p);
     a.max_rounds = 1 << 20;
     seed_kernel<DT><<<m, 128, 0, stream>>>(a, d_sip, d_sdp, d_ns);
-    const RelaxLaunch R = relax_launch<DT>(smem);
+    const RelaxLaunch R = relax_launch<DT>(smem, tiles);
     if (R.resident <= 0) { t_err = "relax kernel cannot be resident"; return -1; }
     // a round visits each queued tile once: more blocks than tiles would only wait at the grid barriers
     const int blocks = int(std::min<size_t>(size_t(R.resident), std::max<size_t>(tiles, 1)));
@@ -1381,7 +1385,7 @@ int na_run(pcbg_search* q, unsigned char* base, cudaStream_t stream) {
                                           reinterpret_cast<const uint64_t* const*>(small + NA_SPTR + 8),
                                           reinterpret_cast<const int*>(small + NA_SPTR + 16));
     const size_t smem = S.mode ? layout(q->nl, joint_wbytes(S.K), 4).total : layout(q->nl, 4, sizeof(DT)).total;
-    const RelaxLaunch R = relax_launch<DT>(smem);
+    const RelaxLaunch R = relax_launch<DT>(smem, tiles);
     const int blocks = R.resident;
     if (blocks <= 0) { na_error("relax kernel cannot be resident%s"); return -1; }
     void* args[] = {&a};
