@@ -118,6 +118,24 @@ def test_batch_matches_oracle(gpu):
         assert np.array_equal(got.view(np.uint32), field.view(np.uint32)), k
 
 
+def test_large_batch_matches_oracle(gpu):
+    """A batch of at least 48 tiles per SM: the solver then runs its 3-blocks-per-SM build of the relax kernel (taken
+    for batches of 16 or more tiles per resident block), which smaller batches never reach."""
+    torch = _torch()
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    side = 960                                     # 30 x 30 tiles per search
+    n = -(-48 * sms // (30 * 30)) + 1
+    searches = [make_device_search(9500 + k, side, side, 2, 20.0) for k in range(n)]
+    arr = run_batch(searches)
+    for k, s in enumerate(searches):
+        field, best, bd = oracle_of(s)
+        assert arr[k].best == best, (k, arr[k].best, best)
+        if best >= 0:
+            assert arr[k].best_d == bd
+        got = s["out"].cpu().numpy().reshape(s["nl"], s["rh"], s["rw"])
+        assert np.array_equal(got.view(np.uint32), field.view(np.uint32)), k
+
+
 def test_walkback_matches_oracle(gpu):
     """The device walk-back (one warp per search, after the relaxation) equals the oracle's walk over its exact
     field: the same states in the same order, best target first, ending on the start."""
