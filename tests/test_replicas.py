@@ -1,4 +1,4 @@
-"""The multi-GPU path of bench.py (replicas, no collective on the data path) on CPU: two gloo ranks take disjoint
+"""The multi-GPU path of bench.py (replicas, no collective on the data path) on CPU: 2 and 4 gloo ranks take disjoint
 round-robin shares of the waves that cover them all, and the timing reduction gives the slowest rank's time and
 the summed work."""
 import os
@@ -30,8 +30,8 @@ def _rank(rank, ws, port, q):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("ws", [2])
-def test_two_gloo_ranks_share_waves_and_reduce_timing(ws):
+@pytest.mark.parametrize("ws", [2, 4])
+def test_gloo_ranks_share_waves_and_reduce_timing(ws):
     import torch.multiprocessing as mp
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
@@ -44,8 +44,10 @@ def test_two_gloo_ranks_share_waves_and_reduce_timing(ws):
         p.join(timeout=60)
         assert p.exitcode == 0
     shares = [set(r[1]) for r in res]
-    assert shares[0].isdisjoint(shares[1])
-    assert shares[0] | shares[1] == set(range(8))
+    for i in range(ws):
+        for j in range(i + 1, ws):
+            assert shares[i].isdisjoint(shares[j])
+    assert set().union(*shares) == set(range(8))
     for r in res:
         assert r[2] == 10.0 * ws          # the slowest rank's time
         assert r[3] == 100 * 8            # all waves' work
