@@ -38,12 +38,14 @@ SEED = 20261203
 WORKLOAD = ("batched-search microbenchmark: 4096 seeded single-source single-target searches, windows log-uniform "
             "64-2048 cells per side, 2-6 layers, cost 1-16 per cell, 15% blocked in value-noise blobs, via cost "
             "8-32; one step = one wave of 512 searches in one persistent launch")
-BYTES_PER_LAYER_VISIT = 32 * 32 * 13     # per staged layer of a tile: cf 4 + flags 1 + distance read 4 + write 4
-BYTES_PER_TILE_VISIT = 32 * 32 * 4       # per tile: via cost of each cell
-# DRAM bytes moved per algorithmic byte by relax_kernel, from one ncu capture of the 64-search case
-# (dram__bytes_read.sum + dram__bytes_write.sum = 11.56 GB against 12.37 GB algorithmic). A full wave is too large to
-# capture; its traffic grows with the tile visits, so the bench scales this ratio by the launch's algorithmic bytes.
-NCU_TRAFFIC_PER_ALG_BYTE = 0.935
+# Algorithmic bytes of the relaxation: 12 per state visit (a 32-bit cost read, a 32-bit distance read and write),
+# where a tile visit stages 32 x 32 states of each of its search's layers. The per-solved-state figure counts the
+# same 12 bytes once per state of the windows solved.
+BYTES_PER_STATE_VISIT = 12
+# DRAM bytes moved per algorithmic byte by relax_kernel, from one ncu capture of the 64-search case (profiles/
+# relax_kernel_microbench.md). A full wave is too large to capture; its traffic grows with the state visits, so the
+# bench scales this ratio by the launch's algorithmic bytes.
+NCU_TRAFFIC_PER_ALG_BYTE = 1.11
 
 
 def peaks():
@@ -178,35 +180,48 @@ def dist_setup():
 
 # ------------------------------------------------------------------------------------------------- CPU baseline
 
-def cpu_solve_sample(sizes, budget_s: float, threads: int, max_searches: int):
-    """Solve searches of the workload in order on the host (exact Dijkstra, `threads` threads) until budget_s of
-    work or max_searches. Returns (states, seconds, searches)."""
+CPU_SAMPLE = 128    # searches of the CPU sample: the first 128 of the workload (197 M states)
+
+
+def config_of(args):
+    """The workload configuration, identical in both arms."""
+    return {"workload": WORKLOAD, "searches": args.searches, "wave": args.wave, "seed": SEED}
+
+
+def cpu_sample(sizes, n):
+    """The first n searches of the workload as dense host arrays, generated by numpy (synth.search_arrays, the same
+    integer hash as the device generator; no CUDA library is loaded), longest first: the host threads take them in
+    that order, so the largest searches start first."""
+    from concurrent.futures import ThreadPoolExecutor
+    from pcbroute_b200 import synth
+
+    def gen(sz):
+        rw, rh, nl, via, sseed = sz
+        cf, fl, vcf, src, tgt = synth.search_arrays(sseed, rw, rh, nl, via)
+        return dict(fac=synth.microbench_factors(nl), cf=cf, flags=fl, vcf=vcf,
+                    start_idx=np.array([src] if src >= 0 else [], np.uint32),
+                    start_d=np.zeros(1 if src >= 0 else 0, np.uint64), states=rw * rh * nl)
+
+    with ThreadPoolExecutor(os.cpu_count() or 1) as ex:
+        batch = list(ex.map(gen, sizes[:n]))
+    batch.sort(key=lambda b: -b["states"])
+    return batch
+
+
+def cpu_solve(batch, threads):
+    """One pass of the exact Dijkstra (oracle/pcb_oracle.c, stopping at the best target as the device solve does)
+    over the sample on `threads` host threads. Returns (window states, reported states, seconds)."""
     from oracle import oracle
-    from pcbroute_b200 import _lib, synth
-    lib = _lib.load()
-    done_states, secs, n = 0, 0.0, 0
-    chunk = max(threads, 8)
-    k = 0
-    while k < min(len(sizes), max_searches) and secs < budget_s:
-        batch = []
-        for (rw, rh, nl, via, sseed) in sizes[k:k + chunk]:
-            cf = np.empty((nl, rh, rw), np.float32)
-            fl = np.empty((nl, rh, rw), np.uint8)
-            vcf = np.empty((rh, rw), np.float32)
-            st = np.empty(2, np.int64)
-            lib.pcbg_synth_search_host(sseed, rw, rh, nl, via, cf.ctypes.data, fl.ctypes.data, vcf.ctypes.data,
-                                       st.ctypes.data, threads)
-            src = int(st[0])
-            batch.append(dict(fac=synth.microbench_factors(nl), cf=cf, flags=fl, vcf=vcf,
-                              start_idx=np.array([src] if src >= 0 else [], np.uint32),
-                              start_d=np.zeros(1 if src >= 0 else 0, np.uint64), states=rw * rh * nl))
-        t0 = time.perf_counter()
-        oracle.solve_many(batch, threads)
-        secs += time.perf_counter() - t0
-        done_states += sum(b["states"] for b in batch)
-        n += len(batch)
-        k += chunk
-    return done_states, secs, n
+    t0 = time.perf_counter()
+    res = oracle.solve_many(batch, threads)
+    secs = time.perf_counter() - t0
+    return sum(b["states"] for b in batch), sum(r[2] for r in res), secs
+
+
+def cpu_sample_text(batch, threads):
+    return (f"the first {len(batch)} searches of the workload ({sum(b['states'] for b in batch)} window states), "
+            f"generated by numpy, largest first; exact Dijkstra (oracle/pcb_oracle.c) stopping at the best target, "
+            f"{threads} host threads")
 
 
 def run_reference(args):
@@ -215,27 +230,28 @@ def run_reference(args):
         return
     from pcbroute_b200 import synth
     threads = os.cpu_count() or 1
-    sizes = synth.microbench_sizes(SEED, args.searches)
-    # calibrate the per-step sample so that the whole run stays within a few minutes
-    st, secs, n = cpu_solve_sample(sizes, 4.0, threads, args.wave)
-    per_step = max(threads, n)
-    for _ in range(max(0, args.warmup - 1)):
-        cpu_solve_sample(sizes, 1e9, threads, per_step)
-    tot_states, tot_s = 0, 0.0
+    batch = cpu_sample(synth.microbench_sizes(SEED, args.searches), CPU_SAMPLE)
+    for _ in range(args.warmup):
+        cpu_solve(batch, threads)
+    tot_states = tot_low = 0
+    tot_s = 0.0
     for _ in range(args.steps):
-        s, t, _n = cpu_solve_sample(sizes, 1e9, threads, per_step)
-        tot_states += s
-        tot_s += t
+        st, low, secs = cpu_solve(batch, threads)
+        tot_states += st
+        tot_low += low
+        tot_s += secs
     v = 9.0 * tot_states / tot_s / 1e9
-    sample = (f"first {per_step} searches of the workload ({tot_states // max(1, args.steps)} states) per step, "
-              f"exact Dijkstra (oracle/pcb_oracle.c) on {threads} host threads")
     line = {
         "impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(1e3 * tot_s / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "searches": args.searches, "wave": args.wave, "seed": SEED,
-                   "parallelism": f"{threads} host threads"},
-        "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "config": config_of(args),
+        "parallelism": f"{threads} host threads",
+        "reported_states": {"value": round(9.0 * tot_low / tot_s / 1e9, 4), "unit": UNIT,
+                            "states_per_step": tot_low // args.steps,
+                            "definition": "9 x the states at or below each search's best target cost, per second"},
+        "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": cpu_sample_text(batch, threads) + ", one pass per step"},
         "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -256,6 +272,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-spec", action="store_true", help="skip the learned-vs-plain speculative batching A/B")
+    ap.add_argument("--band", type=int, default=None,
+                    help="relaxation round band (pcbg_set_round_band); default: the library's own")
     ap.add_argument("--cost-maps-only", type=int, nargs=2, metavar=("NX", "NY"), default=None,
                     help="only time the cost-map rebuild on an NX x NY x 8 board of 4 classes (a profiling case)")
     args = ap.parse_args()
@@ -273,6 +291,8 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     lib = _lib.load()
+    if args.band is not None:
+        lib.pcbg_set_round_band(args.band)
     if args.cost_maps_only:
         if rank == 0:
             print(json.dumps(cost_map_roofline(lib, peaks()[0], *args.cost_maps_only)))
@@ -325,7 +345,7 @@ def main():
     arrays = [search_array(w) for w in dev_waves]
     states = [sum(s["rw"] * s["rh"] * s["nl"] for s in w) for w in dev_waves]
 
-    iters = [0]
+    iters = [0, 0, 0, 0]
 
     def solve(k):
         arr, _ = arrays[k % len(arrays)]
@@ -333,6 +353,9 @@ def main():
         if rc != 0:
             raise RuntimeError("pcbg_solve_batch failed: " + _lib.last_error())
         iters[0] += lib.pcbg_last_batch_local_iters()
+        iters[1] += lib.pcbg_last_batch_deferred()
+        iters[2] += lib.pcbg_last_batch_dropped()
+        iters[3] += lib.pcbg_last_batch_settled()
         return (lib.pcbg_last_batch_kernel_ms(), lib.pcbg_last_batch_tile_visits(), lib.pcbg_last_batch_layer_visits(),
                 lib.pcbg_last_batch_launches(), lib.pcbg_last_batch_rounds())
 
@@ -347,7 +370,7 @@ def main():
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     kms, tv, lv, launches, rounds, st_done = 0.0, 0, 0, 0, 0, 0
-    iters[0] = 0
+    iters[:] = [0, 0, 0, 0]
     with ClockSampler(local) as clk:
         e0.record(stream)
         for k in range(args.steps):
@@ -365,9 +388,12 @@ def main():
     ms = e0.elapsed_time(e1)
     ms_max, states_all = replicas.max_time_sum_work(ms, st_done, "cuda", ws)
     value = 9.0 * states_all / (ms_max / 1e3) / 1e9
-    alg_bytes = lv * BYTES_PER_LAYER_VISIT + tv * BYTES_PER_TILE_VISIT
+    settled_max, settled_all = replicas.max_time_sum_work(ms, iters[3], "cuda", ws)
+    alg_bytes = BYTES_PER_STATE_VISIT * 1024 * lv
+    solved_bytes = BYTES_PER_STATE_VISIT * st_done
     peak, peak_kind = peaks()
     achieved = alg_bytes / (kms / 1e3) / 1e9 if kms > 0 else 0.0
+    achieved_solved = solved_bytes / (kms / 1e3) / 1e9 if kms > 0 else 0.0
 
     # ---- end to end: host (pinned) inputs -> device, solve, reported fields -> host, every step
     e2e = None
@@ -475,27 +501,40 @@ def main():
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        cst, csecs, cn = cpu_solve_sample(sizes, args.cpu_budget, threads, args.wave)
+        batch = cpu_sample(sizes, CPU_SAMPLE)
+        cst, clow, csecs = cpu_solve(batch, threads)
         cv = 9.0 * cst / csecs / 1e9
         cpu = {"value": round(cv, 4), "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"first {cn} searches of the workload ({cst} states), exact Dijkstra "
-                         f"(oracle/pcb_oracle.c) on {threads} host threads, {csecs:.1f} s"}
+               "sample": cpu_sample_text(batch, threads) + f", one pass, {csecs:.1f} s",
+               "reported_states_value": round(9.0 * clow / csecs / 1e9, 4)}
+        del batch
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "searches": args.searches, "wave": args.wave, "seed": SEED,
-                       "states_per_step": int(states_all / args.steps), "parallelism": f"replicas x{ws}",
-                       "l2": "inputs larger than L2 (several GB per wave)",
-                       "tile_visits_per_step": tv // args.steps, "rounds_per_step": rounds // args.steps,
-                       "state_visits_per_state": round(lv * 1024 / max(1, st_done), 3),
-                       "local_iters_per_visit": round(iters[0] / max(1, tv), 3)},
+            "config": config_of(args),
+            "parallelism": f"replicas x{ws}",
+            "l2": "inputs larger than L2 (several GB per wave)",
+            "reported_states": {"value": round(9.0 * settled_all / (ms_max / 1e3) / 1e9, 4), "unit": UNIT,
+                                "states_per_step": int(settled_all // args.steps),
+                                "definition": "9 x the states at or below each search's best target cost, per second"},
+            "kernel_stats": {"states_per_step": int(states_all / args.steps),
+                             "tile_visits_per_step": tv // args.steps, "rounds_per_step": rounds // args.steps,
+                             "state_visits_per_state": round(lv * 1024 / max(1, st_done), 3),
+                             "local_iters_per_visit": round(iters[0] / max(1, tv), 3),
+                             "round_band": int(lib.pcbg_round_band()),
+                             "tiles_deferred_per_step": iters[1] // args.steps,
+                             "tiles_dropped_per_step": iters[2] // args.steps},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4),
                          "traffic": round(NCU_TRAFFIC_PER_ALG_BYTE * alg_bytes / args.steps / 1e9, 2),
                          "traffic_unit": "GB per launch (ncu ratio of the 64-search case x algorithmic bytes)",
+                         "algorithmic_bytes": "12 B per state visit (tile visits x 32 x 32 x the search's layers)",
+                         "per_solved_state": {"achieved": round(achieved_solved, 1),
+                                              "frac": round(achieved_solved / peak, 4),
+                                              "algorithmic_bytes": "12 B per state of the windows solved"},
                          "kernel": "relax_kernel (persistent tile relaxation)",
                          "kernel_ms_per_step": round(kms / args.steps, 3), "peak_kind": peak_kind},
             "gpu_launches": int(launches),

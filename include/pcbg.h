@@ -157,6 +157,47 @@ int32_t pcbg_last_batch_rounds(void);
 float pcbg_last_batch_kernel_ms(void);
 int32_t pcbg_last_batch_launches(void);
 int64_t pcbg_last_batch_local_iters(void);   /* sum over tile visits of local relaxation iterations */
+/* Ordered rounds of the last batch: tiles listed for a round and passed on to a later one, and tiles dropped because
+ * every improvement that listed them lies above the search's best target. */
+int64_t pcbg_last_batch_deferred(void);
+int64_t pcbg_last_batch_dropped(void);
+/* States the last batch reported: at or below each search's best target's cost (every reached state of a search
+ * that reached no target). */
+int64_t pcbg_last_batch_settled(void);
+
+/* Scheduling of the relaxation rounds (no reference counterpart; the reference sweeps whole windows, src/gpu.cu:
+ * 493-524). A queued tile carries the least distance among the edge improvements that queued it; with band B > 0 a
+ * round of a search visits only the tiles keyed within B weight scales of the least key queued for it (the weight
+ * scale: the mean straight-move weight of the search's cheapest well-filled tile), defers the rest to a later round
+ * and drops tiles keyed above the best target found. B = 0 visits every queued tile each round. Results are the
+ * same for every B; only the work changes. Default 16. */
+void pcbg_set_round_band(int32_t band);
+int32_t pcbg_round_band(void);
+/* Cap on the relaxation rounds of one launch (default 2^20; a value < 1 restores it). A launch that reaches the cap
+ * stops and its solve returns PCBG_ERR_FAIL: a bounded device loop, which tests lower to see the error path. */
+void pcbg_set_max_rounds(int32_t rounds);
+
+/* ---- device mirror of the router's cost grids (extends src/gpu.h; replaces the per-solve uploads of
+ * src/gpu.cu:432-439) -----------------------------------------------------------------------------------------------
+ * A router that reports its cost-grid changes keeps a copy of each net class's grids in HBM; gpu_solve / pcbg_solve
+ * then copy a search's rectangle device to device instead of from host memory. The grids are the router's own host
+ * arrays (RClass, src/router.cpp:197-211), layer-major [l][j * nx + i]; the back end page-locks them in place and
+ * remembers the pointers, which must stay valid while the class is mirrored.
+ *   pcbg_mirror_class   after rebuild_costs (src/router.cpp:409-420): every grid of class cls is copied up (the
+ *                       owner grids st / vst on the first call only: they do not change after set-up). oc / ov /
+ *                       hist may be NULL (only the learned scheduler's features read them).
+ *   pcbg_mirror_spans   after refresh_costs(id, spans) (src/router.cpp:1880-1890): the cells of the spans (j, i0, i1
+ *                       triples) of cost grid kind 0 (cst[layer]) or 1 (vcst), and of the occupancy grid the stamp
+ *                       changed (oc[layer] / ov[layer]), are copied up. A class that is not mirrored is ignored.
+ *   pcbg_mirror_history after count_conflicts marked history (src/router.cpp:1970-1999).
+ * Each call returns once the device copy is current. Returns 0 or PCBG_ERR_FAIL. */
+int pcbg_mirror_class(int32_t cls, int32_t nx, int32_t ny, int32_t nl, const float* const* cst, const float* vcst,
+                      const uint16_t* const* st, const uint16_t* vst, const uint8_t* const* oc,
+                      const uint8_t* const* ov, const float* const* hist);
+int pcbg_mirror_spans(int32_t cls, int32_t kind, int32_t layer, const int32_t* spans, int32_t nspans);
+int pcbg_mirror_history(int32_t cls);
+/* The mirrored cost grids of a class, for checks: cst [nl][ny * nx], vcst, oc, ov [nl][ny * nx] (any may be NULL). */
+int pcbg_mirror_download(int32_t cls, float* cst, float* vcst, uint8_t* oc, uint8_t* ov);
 
 /* ---- the round batcher (no reference counterpart) -----------------------------------------------------------
  * pcbg_solve / gpu_solve calls that run concurrently, from the router's worker threads (src/router.cpp:2187-2235
@@ -281,6 +322,38 @@ int pcbg_sched_forward_host(pcbg_sched* s, const uint16_t* x, int32_t B, float* 
 /* Gradients of sum_b w_b BCE(z_b, y_b) / sum_b w_b, packed like the parameters, and that loss. */
 int pcbg_sched_grad_host(pcbg_sched* s, const uint16_t* x, const float* y, const float* w, int32_t B, float* grad,
                          float* loss);
+
+/* Append labelled pairs (x: n rows of PCBG_SCHED_FEATURES bf16 bit patterns, y: n labels 0 / 1) to the
+ * scheduler's conflict log, e.g. the logs a router wrote in log mode (below), before pcbg_sched_train. */
+int pcbg_sched_add_log_host(pcbg_sched* s, const uint16_t* x, const float* y, int64_t n);
+
+/* ---- the learned scheduler inside pcbroute's own router (route_waves, src/router.cpp:2119-2242) -------------
+ * A router built with the hooks of baseline/router_hooks.h calls these from route_waves (no reference
+ * counterpart: the reference takes the next net whenever a worker is free, src/router.cpp:2172-2178). Positions are
+ * places in the call's commit order. The mode comes from the environment: PCBG_SCHED=log with PCBG_SCHED_LOG=<file>
+ * appends the labelled (searched net, uncommitted earlier net) pairs of every speculative search to the file
+ * (records: int64 rows, rows x PCBG_SCHED_FEATURES bf16, rows u8 labels); PCBG_SCHED=learned with
+ * PCBG_SCHED_MODEL=<file> (pcbg_sched_get_params' floats) defers a speculative search while its predicted risk is at
+ * or above PCBG_SCHED_THRESHOLD (default 0.5). Anything else: off, the router's own choice. Features are read from
+ * the mirrored grids of class 0 (pcbg_mirror_class). */
+typedef struct pcbg_rnet {
+    int32_t x0, y0, x1, y1;     /* the net's search window on the board, in cells: [x0, x1) x [y0, y1) */
+    float sx, sy, tx, ty;       /* two pin positions, in cells */
+} pcbg_rnet;
+typedef struct pcbg_rsched_stats {
+    int64_t calls, searches, speculative, commits, wasted, scored, deferred, logged, positives;
+} pcbg_rsched_stats;
+int32_t pcbg_rsched_mode(void);                       /* 0 off, 1 log, 2 learned */
+void pcbg_rsched_begin(int32_t n);                    /* a route_waves call over n nets */
+void pcbg_rsched_net(int32_t pos, const pcbg_rnet* net);
+/* 1 if a worker may search position pos now (the commit point is `cursor`, `version` commits were made). */
+int32_t pcbg_rsched_allow(int32_t pos, int32_t cursor, int64_t version);
+void pcbg_rsched_started(int32_t pos, int32_t cursor, int64_t version);
+void pcbg_rsched_committed(int32_t pos, int64_t commit_index);
+/* The verdict on position pos's search: accepted, and which commits made since it started changed a block it read. */
+void pcbg_rsched_verdict(int32_t pos, int32_t accepted, const int64_t* hit_commits, int32_t nhit);
+void pcbg_rsched_end(void);
+void pcbg_rsched_get_stats(pcbg_rsched_stats* out);
 
 /* ---- seeded synthetic search generator (the batched-search microbenchmark workload) ----------------------- */
 

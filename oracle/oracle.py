@@ -23,7 +23,7 @@ class _Search(C.Structure):
         ("fac", (C.c_float * 8) * 8),
         ("cf", C.c_void_p), ("flags", C.c_void_p), ("vcf", C.c_void_p),
         ("n_starts", C.c_int64), ("start_idx", C.c_void_p), ("start_d", C.c_void_p),
-        ("best", C.c_int64), ("best_d", C.c_uint64),
+        ("best", C.c_int64), ("best_d", C.c_uint64), ("settled", C.c_int64),
     ]
 
 
@@ -144,9 +144,10 @@ def report(dist: np.ndarray, best: int, best_d: int) -> np.ndarray:
     return out
 
 
-def solve_many(searches: list[dict], threads: int) -> list[tuple[int, int]]:
-    """Solve resolved dense searches on host threads. Each dict: fac, cf, flags, vcf, start_idx, start_d.
-    Returns (best, best_d) per search."""
+def solve_many(searches: list[dict], threads: int) -> list[tuple[int, int, int]]:
+    """Solve resolved dense searches on host threads (taken in list order). Each dict: fac, cf, flags, vcf,
+    start_idx, start_d. Returns (best, best_d, settled) per search: settled counts the states at or below best_d
+    (every reached state when no target is reached)."""
     arr = (_Search * len(searches))()
     keep = []
     for k, s in enumerate(searches):
@@ -167,7 +168,7 @@ def solve_many(searches: list[dict], threads: int) -> list[tuple[int, int]]:
         a.vcf = None if vcf is None else vcf.ctypes.data
         a.n_starts, a.start_idx, a.start_d = len(si), si.ctypes.data, sd.ctypes.data
     lib().pcbo_solve_many(arr, len(searches), threads)
-    return [(int(arr[k].best), int(arr[k].best_d)) for k in range(len(searches))]
+    return [(int(arr[k].best), int(arr[k].best_d), int(arr[k].settled)) for k in range(len(searches))]
 
 
 def costs_rebuild(st, oc, ov, vst, hist, gnd, pres: float, hard: bool):

@@ -4,6 +4,7 @@
 // back end": the router-level oracle against which the B200 build's sessions are compared byte for byte.
 #include "gpu.h"
 
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
 #include <vector>
@@ -35,8 +36,29 @@ float GpuOut::operator()(int64_t q) const {
     return d[(size_t(l) * rh + j) * rw + i];
 }
 
+// The back end's host-side fault injection, restated: PCBG_FAIL_SOLVE=k[:p] fails the k-th call (and every p-th
+// after it), so the oracle router and the B200 router fall back to the CPU search on the same searches.
+struct FailPlan {
+    long long first = 0, every = 0;
+    FailPlan() {
+        if (const char* e = std::getenv("PCBG_FAIL_SOLVE")) {
+            char* end = nullptr;
+            first = std::strtoll(e, &end, 10);
+            if (end && *end == ':') every = std::strtoll(end + 1, nullptr, 10);
+        }
+    }
+};
+static std::atomic<long long> g_calls{0};
+static bool injected_failure() {
+    static const FailPlan plan;
+    if (plan.first <= 0) return false;
+    const long long n = ++g_calls;
+    return n == plan.first || (plan.every > 0 && n > plan.first && (n - plan.first) % plan.every == 0);
+}
+
 int gpu_solve(const GpuQuery& q, GpuOut& out, bool wait) {
     (void)wait;
+    if (injected_failure()) return -1;
     if (q.NL < 1 || q.NL > 8) return -1;
     auto flat = [](const std::vector<std::pair<uint32_t, float>>& v, std::vector<uint32_t>& i, std::vector<float>& x) {
         for (const auto& p : v) { i.push_back(p.first); x.push_back(p.second); }

@@ -154,9 +154,15 @@ int64_t pcbo_dijkstra(int rw, int rh, int nl, const float fac[8][8], const float
         if (s >= N) continue;
         if (start_d[k] < dist[s]) { dist[s] = start_d[k]; hpush(&h, start_d[k], s); }
     }
+    /* Early exit at the best target, as the device solve: once a target is popped at distance D, every state at or
+     * below D is exact when the pops pass D (ties included), and nothing above D is reported. States above D keep
+     * their tentative distances (upper bounds, never below the exact ones). */
+    uint64_t bound = PCBO_INF64;
     while (h.n) {
         hitem it = hpop(&h);
         if (it.d != dist[it.s]) continue;
+        if (it.d > bound) break;
+        if ((flags[it.s] & 2) && bound == PCBO_INF64) bound = it.d;
         const uint32_t s = it.s;
         const int l = (int)(s / RN);
         const size_t c = s % RN;
@@ -367,6 +373,11 @@ static void* many_worker(void* arg) {
         uint64_t* dist = (uint64_t*)malloc(N * sizeof(uint64_t));
         s->best = pcbo_dijkstra(s->rw, s->rh, s->nl, (const float(*)[8])s->fac, s->cf, s->flags, s->vcf, s->n_starts,
                                 s->start_idx, s->start_d, dist, &s->best_d);
+        /* the states a solve reports: at or below the best target's cost (every reached state when none) */
+        const uint64_t lim = s->best >= 0 ? s->best_d : PCBO_INF64 - 1;
+        int64_t settled = 0;
+        for (size_t q = 0; q < N; ++q) settled += dist[q] <= lim;
+        s->settled = settled;
         free(dist);
     }
     return NULL;

@@ -43,7 +43,8 @@ void pcbo_resolve(const pcbg_query* q, int rx0, int ry0, int rw, int rh, float* 
 
 /* Exact least fixed point over a resolved dense rectangle. starts: rect states and fixed-point costs (the least
  * per state counts). dist: nl*rh*rw 64-bit distances (PCBO_INF64 unreached). Returns best rect state or -1, and
- * its cost in *best_d. */
+ * its cost in *best_d. When a target is reached, the search stops once it has settled every state at or below the
+ * target's cost (the part of the field a solve reports); states above it keep upper bounds. */
 int64_t pcbo_dijkstra(int rw, int rh, int nl, const float fac[8][8], const float* cf, const uint8_t* flags,
                       const float* vcf, int64_t n_starts, const uint32_t* start_idx, const uint64_t* start_d,
                       uint64_t* dist, uint64_t* best_d);
@@ -87,8 +88,9 @@ typedef struct pcbo_search {
     const uint64_t* start_d;
     int64_t best;
     uint64_t best_d;
+    int64_t settled;            /* states at or below best_d (every reached state when no target is reached) */
 } pcbo_search;
-/* Solve n searches on `threads` host threads (one search per thread at a time). */
+/* Solve n searches on `threads` host threads (one search per thread at a time, taken in array order). */
 void pcbo_solve_many(pcbo_search* s, int n, int threads);
 
 #ifdef __cplusplus

@@ -22,6 +22,11 @@ PCBG_SYMBOLS = [
     "pcbg_sched_log_size", "pcbg_sched_train", "pcbg_sched_counts", "pcbg_sched_nparams", "pcbg_sched_get_params",
     "pcbg_sched_set_params", "pcbg_sched_forward_host", "pcbg_sched_grad_host", "pcbg_last_batch_tile_visits", "pcbg_last_batch_layer_visits", "pcbg_last_batch_rounds",
     "pcbg_last_batch_kernel_ms", "pcbg_last_batch_launches", "pcbg_last_batch_local_iters", "pcbg_synth_search",
+    "pcbg_last_batch_deferred", "pcbg_last_batch_dropped", "pcbg_set_round_band", "pcbg_round_band",
+    "pcbg_set_max_rounds", "pcbg_last_batch_settled", "pcbg_mirror_class", "pcbg_mirror_spans",
+    "pcbg_mirror_history", "pcbg_mirror_download", "pcbg_sched_add_log_host", "pcbg_rsched_mode",
+    "pcbg_rsched_begin", "pcbg_rsched_net", "pcbg_rsched_allow", "pcbg_rsched_started", "pcbg_rsched_committed",
+    "pcbg_rsched_verdict", "pcbg_rsched_end", "pcbg_rsched_get_stats",
     "pcbg_synth_search_host", "pcbg_costs_create", "pcbg_costs_destroy", "pcbg_costs_set_static",
     "pcbg_costs_set_occupancy", "pcbg_costs_set_history", "pcbg_costs_set_ground", "pcbg_costs_rebuild",
     "pcbg_costs_stamp", "pcbg_costs_add_history", "pcbg_costs_download", "pcbg_costs_download_history",
@@ -134,6 +139,24 @@ def load() -> C.CDLL:
     lib.pcbg_last_batch_kernel_ms.restype = C.c_float
     lib.pcbg_last_batch_launches.restype = C.c_int32
     lib.pcbg_last_batch_local_iters.restype = C.c_int64
+    lib.pcbg_last_batch_deferred.restype = C.c_int64
+    lib.pcbg_last_batch_dropped.restype = C.c_int64
+    lib.pcbg_last_batch_settled.restype = C.c_int64
+    lib.pcbg_mirror_class.argtypes = [C.c_int32] * 4 + [C.c_void_p] * 7
+    lib.pcbg_mirror_class.restype = C.c_int
+    lib.pcbg_mirror_spans.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int32]
+    lib.pcbg_mirror_spans.restype = C.c_int
+    lib.pcbg_mirror_history.argtypes = [C.c_int32]
+    lib.pcbg_mirror_history.restype = C.c_int
+    lib.pcbg_mirror_download.argtypes = [C.c_int32] + [C.c_void_p] * 4
+    lib.pcbg_mirror_download.restype = C.c_int
+    lib.pcbg_sched_add_log_host.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64]
+    lib.pcbg_sched_add_log_host.restype = C.c_int
+    lib.pcbg_set_round_band.argtypes = [C.c_int32]
+    lib.pcbg_set_round_band.restype = None
+    lib.pcbg_round_band.restype = C.c_int32
+    lib.pcbg_set_max_rounds.argtypes = [C.c_int32]
+    lib.pcbg_set_max_rounds.restype = None
     lib.pcbg_spec_create.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_float]
     lib.pcbg_spec_create.restype = C.c_void_p
     lib.pcbg_spec_destroy.argtypes = [C.c_void_p]

@@ -24,7 +24,8 @@ ORACLE_LIB = os.path.join(ORACLE_DIR, "_build", "libpcboracle.so")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["solver.cu", "query.cu", "batcher.cpp", "synth.cu", "costs.cu", "spec.cu", "mlp.cu", "sched.cu", "gpu_api.cpp"]
+SOURCES = ["solver.cu", "query.cu", "batcher.cpp", "synth.cu", "costs.cu", "spec.cu", "mlp.cu", "sched.cu", "mirror.cu",
+           "gpu_api.cpp"]
 
 
 def _run(cmd: list[str]) -> None:

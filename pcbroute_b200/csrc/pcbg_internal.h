@@ -40,6 +40,7 @@ struct SDev {
     void* dist;
     uint32_t* stamp;
     uint32_t* sides;   // per tile: which halo sides changed since its last visit (bit 8: everything)
+    uint32_t* tkey;    // per tile: least improved edge distance that queued it since its last visit (all ones: none)
     float* out;
     uint32_t* path;    // walk-back output (or null), capacity path_cap; its length goes to *path_len
     int* path_len;
@@ -53,7 +54,9 @@ struct SStat {
     unsigned long long best;      // rect state of the cheapest target (all ones: none)
     unsigned long long maxd;      // largest finite distance in the field
     unsigned int need_wide;       // a finite weight does not fit 32-bit arithmetic
-    unsigned int pad;
+    unsigned int wscale;          // least mean straight-move weight over the well-filled tiles visited (all ones: none)
+    unsigned int kmin[3];         // per rotating round: least key of the tiles queued for it (all ones: none)
+    unsigned int settled;         // states reported: at or below the best target's cost (all reached when none)
 };
 
 // Search handed to the batch solver (host side).
@@ -91,6 +94,9 @@ struct BatchStats {
     float kernel_ms = 0.f;         // device time of the relaxation launches (CUDA events on the launch stream)
     int launches = 0;              // kernels this library launched for the batch
     long long local_iters = 0;     // sum over tile visits of the local relaxation iterations
+    long long deferred = 0;        // ordered rounds: tiles listed for a round and passed on to the next one
+    long long dropped = 0;         // ordered rounds: tiles dropped because nothing that queued them can matter
+    long long settled = 0;         // states at or below their search's best target's cost (all reached when none)
 };
 BatchStats& last_stats();
 
@@ -120,6 +126,17 @@ struct CostPlanes {
     const float* hist[MAX_LAYERS];
 };
 bool cost_planes(pcbg_costs* h, int cls, CostPlanes& out);
+
+// The router's cost grids mirrored in device memory (mirror.cu). mirror_lookup: the device planes of the mirrored
+// class whose host grids the query points at (false: not mirrored). mirror_planes: a mirrored class as cost planes.
+struct MirrorView {
+    const float* cst[MAX_LAYERS];
+    const uint16_t* st[MAX_LAYERS];
+    const float* vcst;
+    const uint16_t* vst;
+};
+bool mirror_lookup(const pcbg_query& q, MirrorView& v);
+bool mirror_planes(int cls, CostPlanes& out);
 
 // The conflict predictor's network (mlp.cu): D0 inputs (two 32 x 32 rasters, an 8 x 8 overlap mask, 64 scalars),
 // two hidden layers of MLP_H, one logit. BF16 operands, FP32 accumulation, FP32 master weights under Adam.

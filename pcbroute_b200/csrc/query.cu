@@ -8,6 +8,7 @@
 // target (src/gpu.cu:575-619); the touched-block bookkeeping of the router depends on that rectangle, so the rule
 // is kept as the reference has it.
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cmath>
 #include <cstring>
@@ -204,8 +205,21 @@ int solve_rect(Slot& E, const pcbg_query& q, int rx0, int ry0, int rw, int rh, p
     // the resolve kernel).
     const size_t rows = size_t(rh) * pitch;
     const size_t grid_bytes = rows * 6, total = grid_bytes * size_t(nl + (vias ? 1 : 0));
-    if (!stage_need(E, total)) { set_error("pinned allocation failed"); return -1; }
     const int ngrids = nl + (vias ? 1 : 0);
+    MirrorView mv;
+    const bool mirrored = mirror_lookup(q, mv);
+    if (mirrored) {
+        // the class's grids are in HBM already: the rectangle is copied device to device
+        for (int l = 0; l < ngrids; ++l) {
+            float* dc = l < nl ? E.cf.p + size_t(l) * plane : E.vcf.p;
+            uint16_t* ds = l < nl ? E.st.p + size_t(l) * plane : E.vst.p;
+            const float* sc = (l < nl ? mv.cst[l] : mv.vcst) + hoff;
+            const uint16_t* ss = (l < nl ? mv.st[l] : mv.vst) + hoff;
+            CK(cudaMemcpy2DAsync(dc, size_t(pitch) * 4, sc, size_t(q.nx) * 4, size_t(rw) * 4, rh, cudaMemcpyDeviceToDevice, S));
+            CK(cudaMemcpy2DAsync(ds, size_t(pitch) * 2, ss, size_t(q.nx) * 2, size_t(rw) * 2, rh, cudaMemcpyDeviceToDevice, S));
+        }
+    }
+    if (!mirrored && !stage_need(E, total)) { set_error("pinned allocation failed"); return -1; }
     auto pack = [&](int j0, int j1) {
         for (int l = 0; l < ngrids; ++l) {
             pack_rows(reinterpret_cast<float*>(E.stage + size_t(l) * grid_bytes), l < nl ? q.cst[l] : q.vcst,
@@ -216,7 +230,8 @@ int solve_rect(Slot& E, const pcbg_query& q, int rx0, int ry0, int rw, int rh, p
     };
     // a whole-board rectangle packs tens of MB: split its rows over a few threads
     const int nth = total > (size_t(16) << 20) ? 4 : 1;
-    if (nth == 1) {
+    if (mirrored) {
+    } else if (nth == 1) {
         pack(0, rh);
     } else {
         std::vector<std::thread> th;
@@ -224,7 +239,7 @@ int solve_rect(Slot& E, const pcbg_query& q, int rx0, int ry0, int rw, int rh, p
         pack(0, rh / nth);
         for (auto& x : th) x.join();
     }
-    for (int l = 0; l < ngrids; ++l) {
+    for (int l = 0; l < ngrids && !mirrored; ++l) {
         float* hc = reinterpret_cast<float*>(E.stage + size_t(l) * grid_bytes);
         uint16_t* hs = reinterpret_cast<uint16_t*>(E.stage + size_t(l) * grid_bytes + rows * 4);
         float* dc = l < nl ? E.cf.p + size_t(l) * plane : E.vcf.p;
@@ -393,7 +408,32 @@ extern "C" void pcbg_host_release(float* p, size_t cap) {
     g_pool.push_back({p, cap});
 }
 
+// Host-side fault injection, for tests of the caller's fallback (the router carries on with its CPU search when
+// gpu_solve returns -1, src/router.cpp:1598, 1691-1700). PCBG_FAIL_SOLVE=k makes the k-th call of this process
+// (counting from 1) fail before it touches the device; PCBG_FAIL_SOLVE=k:p also fails every p-th call after it.
+// Nothing is injected on the device.
+namespace {
+struct FailPlan {
+    long long first = 0, every = 0;
+    FailPlan() {
+        const char* e = std::getenv("PCBG_FAIL_SOLVE");
+        if (!e) return;
+        char* end = nullptr;
+        first = std::strtoll(e, &end, 10);
+        if (end && *end == ':') every = std::strtoll(end + 1, nullptr, 10);
+    }
+};
+std::atomic<long long> g_solve_calls{0};
+bool injected_failure() {
+    static const FailPlan plan;
+    if (plan.first <= 0) return false;
+    const long long n = ++g_solve_calls;
+    return n == plan.first || (plan.every > 0 && n > plan.first && (n - plan.first) % plan.every == 0);
+}
+}  // namespace
+
 extern "C" int pcbg_solve(const pcbg_query* qp, pcbg_result* out, int wait) {
+    if (injected_failure()) { set_error("injected failure (PCBG_FAIL_SOLVE)"); return PCBG_ERR_FAIL; }
     if (!pcbg_available()) { set_error("no usable device"); return PCBG_ERR_FAIL; }
     const pcbg_query& q = *qp;
     if (q.nl < 1 || q.nl > MAX_LAYERS || q.ww < 1 || q.wh < 1) { set_error("bad query"); return PCBG_ERR_FAIL; }

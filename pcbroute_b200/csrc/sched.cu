@@ -18,7 +18,10 @@
 // paths. Training runs the MLP's own forward and backward kernels (mlp.cu) with Adam, on the GPU.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -438,4 +441,249 @@ extern "C" int pcbg_sched_grad_host(pcbg_sched* S, const uint16_t* x, const floa
     if (rc == 0 && cudaMemcpyAsync(grad, S->net.grad, S->net.nparams * 4, cudaMemcpyDeviceToHost, S->stream) != cudaSuccess) rc = -1;
     if (cudaStreamSynchronize(S->stream) != cudaSuccess) rc = -1;
     return rc == 0 ? 0 : PCBG_ERR_FAIL;
+}
+
+// ---- the learned scheduler inside pcbroute's own router (route_waves, src/router.cpp:2119-2242) ----
+//
+// The router's worker takes the next net of the commit order within the lookahead (src/router.cpp:2172-2178); a
+// search is wasted when a commit made after it started changes a 16 x 16 block it read (src/router.cpp:2200-2216).
+// A router built with the hooks (baseline/router_hooks.h) reports, per route_waves call, each net's search window
+// and pins, the start of each search, each commit and each verdict. In log mode the scheduler records the features
+// of every (searched net, uncommitted earlier net) pair at search start and labels them at the verdict: positive
+// when the earlier net's commit changed a block the search read. In learned mode it lets a worker start net i ahead
+// of the commit point only while the predicted risk 1 - prod_j (1 - p_ij) stays below the threshold; the net at
+// the commit point is always searched, and the commit order and check are the router's own, so the session cannot
+// change. Mode, model and log files come from the environment:
+//   PCBG_SCHED=log|learned, PCBG_SCHED_LOG=<file> (log mode: labelled pairs appended), PCBG_SCHED_MODEL=<file>
+//   (learned mode: parameters as written by pcbg_sched_get_params), PCBG_SCHED_THRESHOLD (default 0.5).
+
+namespace {
+
+constexpr int RBS = 16;   // the router's block side (src/router.cpp:404)
+
+struct RPair {
+    int i, j;
+    int64_t row;   // row of the pending log
+};
+
+struct RSched {
+    std::mutex mu;
+    int mode = -1;             // 0 off, 1 log, 2 learned
+    float threshold = 0.5f;
+    std::string log_path;
+    pcbg_sched* S = nullptr;
+    std::vector<pcbg_rnet> nets;
+    std::vector<int64_t> commit_of;   // per position: index of the commit that committed it (-1: none yet)
+    std::vector<RPair> pending;       // logged pairs awaiting their verdict
+    __nv_bfloat16* X = nullptr;       // pending features (device)
+    size_t xcap = 0, nx_rows = 0;
+    std::vector<uint16_t> out_x;      // labelled rows not yet written
+    std::vector<uint8_t> out_y;
+    int64_t cache_pos = -1, cache_ver = -1, cache_cur = -1;
+    int cache_val = 1;
+    uint64_t rng = 0x9E3779B97F4A7C15ull;
+    pcbg_rsched_stats st{};
+};
+
+RSched g_rs;
+
+void rs_init() {
+    if (g_rs.mode >= 0) return;
+    g_rs.mode = 0;
+    const char* m = std::getenv("PCBG_SCHED");
+    if (!m) return;
+    const std::string mode(m);
+    if (const char* t = std::getenv("PCBG_SCHED_THRESHOLD")) g_rs.threshold = float(std::atof(t));
+    if (mode == "log") {
+        const char* p = std::getenv("PCBG_SCHED_LOG");
+        if (!p) return;
+        g_rs.log_path = p;
+        g_rs.S = pcbg_sched_create(1);
+        if (g_rs.S) g_rs.mode = 1;
+    } else if (mode == "learned") {
+        const char* p = std::getenv("PCBG_SCHED_MODEL");
+        if (!p) return;
+        g_rs.S = pcbg_sched_create(1);
+        if (!g_rs.S) return;
+        std::vector<float> w(g_rs.S->net.nparams);
+        FILE* f = std::fopen(p, "rb");
+        if (!f) return;
+        const size_t got = std::fread(w.data(), 4, w.size(), f);
+        std::fclose(f);
+        if (got != w.size() || pcbg_sched_set_params(g_rs.S, w.data()) != 0) return;
+        g_rs.mode = 2;
+    }
+}
+
+bool rs_blocks_meet(const pcbg_rnet& a, const pcbg_rnet& b) {
+    return a.x0 / RBS <= (b.x1 - 1) / RBS && b.x0 / RBS <= (a.x1 - 1) / RBS && a.y0 / RBS <= (b.y1 - 1) / RBS &&
+           b.y0 / RBS <= (a.y1 - 1) / RBS;
+}
+
+PairDesc rs_pair(int i, int j) {
+    const pcbg_rnet &a = g_rs.nets[i], &b = g_rs.nets[j];
+    PairDesc d;
+    d.ix0 = a.x0; d.iy0 = a.y0; d.ix1 = a.x1; d.iy1 = a.y1;
+    d.jx0 = b.x0; d.jy0 = b.y0; d.jx1 = b.x1; d.jy1 = b.y1;
+    d.jsx = b.sx; d.jsy = b.sy; d.jtx = b.tx; d.jty = b.ty;
+    d.gap = float(i - j);
+    return d;
+}
+
+// features of pairs (i, j) for j in js into X (stream-ordered on the scheduler's stream)
+int rs_features(const std::vector<PairDesc>& pds, __nv_bfloat16* X) {
+    CostPlanes P;
+    if (!mirror_planes(0, P)) return -1;
+    pcbg_sched* S = g_rs.S;
+    if (!grow(S->pd, S->pdcap, pds.size())) return -1;
+    cudaMemcpyAsync(S->pd, pds.data(), pds.size() * sizeof(PairDesc), cudaMemcpyHostToDevice, S->stream);
+    pair_features_kernel<<<unsigned(pds.size()), 256, 0, S->stream>>>(P, S->pd, X);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+void rs_flush() {
+    if (g_rs.mode != 1 || g_rs.out_y.empty()) return;
+    FILE* f = std::fopen(g_rs.log_path.c_str(), "ab");
+    if (!f) return;
+    // record: int64 rows, then rows x MLP_D0 bf16, then rows labels (u8)
+    const int64_t rows = int64_t(g_rs.out_y.size());
+    std::fwrite(&rows, 8, 1, f);
+    std::fwrite(g_rs.out_x.data(), 2, g_rs.out_x.size(), f);
+    std::fwrite(g_rs.out_y.data(), 1, g_rs.out_y.size(), f);
+    std::fclose(f);
+    g_rs.out_x.clear();
+    g_rs.out_y.clear();
+}
+
+}  // namespace
+
+extern "C" int pcbg_rsched_mode(void) {
+    std::lock_guard<std::mutex> g(g_rs.mu);
+    rs_init();
+    return g_rs.mode;
+}
+
+extern "C" void pcbg_rsched_begin(int32_t n) {
+    std::lock_guard<std::mutex> g(g_rs.mu);
+    rs_init();
+    g_rs.nets.assign(n > 0 ? n : 0, pcbg_rnet{});
+    g_rs.commit_of.assign(n > 0 ? n : 0, -1);
+    g_rs.pending.clear();
+    g_rs.nx_rows = 0;
+    g_rs.cache_pos = -1;
+    ++g_rs.st.calls;
+}
+
+extern "C" void pcbg_rsched_net(int32_t pos, const pcbg_rnet* net) {
+    std::lock_guard<std::mutex> g(g_rs.mu);
+    if (pos >= 0 && pos < int(g_rs.nets.size()) && net) g_rs.nets[pos] = *net;
+}
+
+extern "C" int32_t pcbg_rsched_allow(int32_t pos, int32_t cursor, int64_t version) {
+    std::lock_guard<std::mutex> g(g_rs.mu);
+    if (g_rs.mode != 2 || pos <= cursor || pos >= int(g_rs.nets.size())) return 1;
+    if (g_rs.cache_pos == pos && g_rs.cache_ver == version && g_rs.cache_cur == cursor) return g_rs.cache_val;
+    std::vector<PairDesc> pds;
+    for (int j = cursor; j < pos; ++j)
+        if (rs_blocks_meet(g_rs.nets[pos], g_rs.nets[j])) pds.push_back(rs_pair(pos, j));
+    int allow = 1;
+    if (!pds.empty()) {
+        pcbg_sched* S = g_rs.S;
+        const size_t B = round_up(pds.size(), 64);
+        if (!grow(S->xb, S->xbcap, B * MLP_D0) || !grow(S->pb, S->pbcap, B)) return 1;
+        cudaMemsetAsync(S->xb, 0, B * MLP_D0 * 2, S->stream);
+        if (rs_features(pds, S->xb) != 0 || S->net.forward(S->stream, S->xb, int(B), S->pb) != 0) return 1;
+        std::vector<float> p(pds.size());
+        cudaMemcpyAsync(p.data(), S->pb, p.size() * 4, cudaMemcpyDeviceToHost, S->stream);
+        if (cudaStreamSynchronize(S->stream) != cudaSuccess) return 1;
+        double keep = 1.0;
+        for (float x : p) keep *= 1.0 - double(x);
+        allow = 1.0 - keep < double(g_rs.threshold) ? 1 : 0;
+        ++g_rs.st.scored;
+        if (!allow) ++g_rs.st.deferred;
+    }
+    g_rs.cache_pos = pos; g_rs.cache_ver = version; g_rs.cache_cur = cursor; g_rs.cache_val = allow;
+    return allow;
+}
+
+extern "C" void pcbg_rsched_started(int32_t pos, int32_t cursor, int64_t version) {
+    (void)version;
+    std::lock_guard<std::mutex> g(g_rs.mu);
+    ++g_rs.st.searches;
+    if (pos > cursor) ++g_rs.st.speculative;
+    if (g_rs.mode != 1 || pos <= cursor || pos >= int(g_rs.nets.size())) return;
+    std::vector<PairDesc> pds;
+    std::vector<int> js;
+    for (int j = cursor; j < pos; ++j)
+        if (rs_blocks_meet(g_rs.nets[pos], g_rs.nets[j])) { pds.push_back(rs_pair(pos, j)); js.push_back(j); }
+    if (pds.empty()) return;
+    if (!grow(g_rs.X, g_rs.xcap, (g_rs.nx_rows + pds.size()) * MLP_D0)) return;
+    if (rs_features(pds, g_rs.X + g_rs.nx_rows * MLP_D0) != 0) return;
+    for (size_t k = 0; k < js.size(); ++k) g_rs.pending.push_back({pos, js[k], int64_t(g_rs.nx_rows + k)});
+    g_rs.nx_rows += pds.size();
+}
+
+extern "C" void pcbg_rsched_committed(int32_t pos, int64_t commit_index) {
+    std::lock_guard<std::mutex> g(g_rs.mu);
+    if (pos >= 0 && pos < int(g_rs.commit_of.size())) g_rs.commit_of[pos] = commit_index;
+    ++g_rs.st.commits;
+}
+
+extern "C" void pcbg_rsched_verdict(int32_t pos, int32_t accepted, const int64_t* hit_commits, int32_t nhit) {
+    std::lock_guard<std::mutex> g(g_rs.mu);
+    if (!accepted) ++g_rs.st.wasted;
+    if (g_rs.mode != 1) return;
+    std::vector<RPair> rest;
+    std::vector<std::pair<int64_t, uint8_t>> lab;
+    for (const RPair& p : g_rs.pending) {
+        if (p.i != pos) { rest.push_back(p); continue; }
+        const int64_t c = p.j < int(g_rs.commit_of.size()) ? g_rs.commit_of[p.j] : -1;
+        bool hit = false;
+        for (int k = 0; k < nhit && !hit; ++k) hit = hit_commits[k] == c;
+        // negatives are sampled (1 in 4) to bound the log; positives are all kept
+        g_rs.rng = g_rs.rng * 6364136223846793005ull + 1442695040888963407ull;
+        if (!hit && (g_rs.rng >> 33) % 4 != 0) continue;
+        lab.push_back({p.row, uint8_t(hit ? 1 : 0)});
+    }
+    g_rs.pending.swap(rest);
+    if (lab.empty()) return;
+    const size_t old = g_rs.out_x.size();
+    g_rs.out_x.resize(old + lab.size() * MLP_D0);
+    cudaStreamSynchronize(g_rs.S->stream);
+    for (size_t k = 0; k < lab.size(); ++k) {
+        cudaMemcpy(g_rs.out_x.data() + old + k * MLP_D0, g_rs.X + size_t(lab[k].first) * MLP_D0, MLP_D0 * 2,
+                   cudaMemcpyDeviceToHost);
+        g_rs.out_y.push_back(lab[k].second);
+        g_rs.st.logged += 1;
+        g_rs.st.positives += lab[k].second;
+    }
+    if (g_rs.out_y.size() >= 4096) rs_flush();
+}
+
+extern "C" void pcbg_rsched_end(void) {
+    std::lock_guard<std::mutex> g(g_rs.mu);
+    rs_flush();
+    g_rs.pending.clear();
+    g_rs.nx_rows = 0;
+}
+
+extern "C" void pcbg_rsched_get_stats(pcbg_rsched_stats* out) {
+    std::lock_guard<std::mutex> g(g_rs.mu);
+    if (out) *out = g_rs.st;
+}
+
+extern "C" int pcbg_sched_add_log_host(pcbg_sched* S, const uint16_t* x, const float* y, int64_t n) {
+    if (n <= 0) return 0;
+    if (S->labelled != S->nlog) { set_error("unlabelled pairs pending"); return PCBG_ERR_FAIL; }
+    if (!grow(S->X, S->xcap, (S->nlog + size_t(n)) * MLP_D0)) return PCBG_ERR_FAIL;
+    if (cudaMemcpy(S->X + S->nlog * MLP_D0, x, size_t(n) * MLP_D0 * 2, cudaMemcpyHostToDevice) != cudaSuccess)
+        return PCBG_ERR_FAIL;
+    for (int64_t k = 0; k < n; ++k) {
+        S->li.push_back(-1);
+        S->lj.push_back(-1);
+        S->label.push_back(y[k]);
+    }
+    S->nlog += size_t(n);
+    S->labelled = S->nlog;
+    return 0;
 }

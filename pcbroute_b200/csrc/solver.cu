@@ -16,15 +16,22 @@
 //   * a tile whose edge cell improved below the staged value of an adjacent cell of a neighbour (and not above the
 //     best target found so far) queues that neighbour for the next round;
 //   * one persistent cooperative launch runs all rounds of all searches of a batch, with a bounded software grid
-//     barrier between rounds, so a whole round of searches with uneven windows and layer counts shares the GPU.
+//     barrier between rounds, so a whole round of searches with uneven windows and layer counts shares the GPU;
+//   * rounds go in distance order per search (delta-stepping at tile granularity): a queued tile carries a key,
+//     the least improved edge distance that queued it, and a round visits only the tiles whose key lies within a
+//     band of the search's least key; the others wait for a later round, and tiles keyed above the search's best
+//     target are dropped. Tiles visited concurrently in one round read each other's old edges, so an unordered
+//     round revisits a tile each time a wave of improvements crosses it; the band keeps the visits near the front.
 //
 // Exactness: distances are fixed-point integers (pcbg.h); min-plus over integers is exact and associative, so the
 // least fixed point is unique and any monotone schedule reaches it. A visit ends only after a full pass changed
 // nothing, and a neighbour is skipped only when no edge value can lower its adjacent cells; improvements above the
-// best target are not propagated (no path through them can matter). The epilogue reports every state at or below
+// best target are not propagated (no path through them can matter), and a queued tile is dropped only when every
+// improvement that queued it lies above the best target. Deferring a tile to a later round changes only the order. The epilogue reports every state at or below
 // the best target's cost, and those are exact.
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -44,9 +51,14 @@ constexpr int WLS = TILE * CSTR;        // weight plane stride (one layer)
 constexpr int MAX_IT = 64;              // local iterations before a tile is re-queued instead
 constexpr long long BAR_SPIN_LIMIT = 1ll << 24;   // polls (with __nanosleep) before a barrier wait gives up
 
-// control words of a batch
-enum { C_CNT = 0, C_NEXT = 3, C_BAR = 6, C_GEN = 7, C_ERR = 8, C_ROUNDS = 9, C_N = 16 };
+constexpr uint32_t KEY_NONE = 0xFFFFFFFFu;   // tile key / round minimum: nothing queued
+
+// control words of a batch: per rotating round the queued count and the next item taken; per round parity the
+// count and next item of the round's visit list (ordered rounds)
+enum { C_CNT = 0, C_NEXT = 3, C_BAR = 6, C_GEN = 7, C_ERR = 8, C_ROUNDS = 9, C_VCNT = 10, C_VNEXT = 12, C_N = 16 };
 enum { ERR_BARRIER = 1, ERR_ROUNDS = 2, ERR_OVERFLOW = 4 };
+// counters of a launch: tile visits, layer visits, local iterations, tiles deferred to a later round, tiles dropped
+constexpr int NVIS = 5;
 
 template <typename DT> struct Lim;
 template <> struct Lim<uint32_t> {
@@ -81,11 +93,19 @@ struct SolveArgs {
     int nlmax;
     int kmax;                     // weight planes of joint-mode searches (0: none in the batch)
     unsigned long long* wl;       // 3 rotating worklists of `cap` items: (search << 32) | tile
+    unsigned long long* vl;       // ordered rounds: the items of the current round that are visited (cap items)
     unsigned int cap;
     unsigned int* ctl;
-    unsigned long long* visits;   // tile visits, layer visits, local iterations
+    unsigned long long* visits;   // NVIS counters
     int max_rounds;
+    int ordered;                  // 1: rounds in distance bands (32-bit distances only), 0: every queued tile
+    unsigned int band;            // band width of an ordered round, in multiples of the search's weight scale
 };
+
+// Key of an improvement: its distance, as 32 bits (64-bit distances run unordered and only need "some key").
+template <typename DT> __device__ __forceinline__ uint32_t key_of(DT v) {
+    return static_cast<unsigned long long>(v) < KEY_NONE ? uint32_t(v) : KEY_NONE - 1;
+}
 
 // Shared memory of a visit. d: distances with halo [nl][HS][DSTR]; w: joint mode, K integer weight planes
 // [K][nl][TILE][CSTR] (general mode: float cost factors [nl][TILE][CSTR]); v: via weight per cell; e: staged edge
@@ -145,9 +165,23 @@ __device__ __forceinline__ void enqueue(const SolveArgs& a, const SDev& S, int s
     else atomicOr(a.ctl + C_ERR, unsigned(ERR_OVERFLOW));
 }
 
+// Queue a tile for next_round with the key of what queued it: the tile's key and the round's least key for the
+// search both take the minimum before the tile is listed (the key counts even when the tile is listed already).
+__device__ __forceinline__ void queue_tile(const SolveArgs& a, const SDev& S, int s, int tile, int next_round,
+                                           uint32_t key) {
+    if (a.ordered) {
+        atomicMin(S.tkey + tile, key);
+        atomicMin(&a.st[s].kmin[next_round % 3], key);
+    }
+    enqueue(a, S, s, tile, next_round);
+}
+
 struct VisitShared {
     unsigned int marks, any, wide, iters, sides;
-    unsigned long long tmin, wmax;
+    unsigned int kvis;             // the tile's key when the visit took it (ordered rounds)
+    unsigned int mkey[8];          // per neighbour marked: least improved edge value that marked it
+    unsigned int wcnt;             // finite straight-move weights staged, and their sum (ordered rounds)
+    unsigned long long tmin, wmax, wsum;
 };
 
 // Halo sides of a tile, as neighbour directions: 0 L, 1 R, 2 T, 3 B, 4 TL, 5 TR, 6 BL, 7 BR; SIDE_ALL: the interior
@@ -636,16 +670,20 @@ __device__ void visit_tile(const SolveArgs& a, int s, int tile, int round, unsig
     const DT INF = Lim<DT>::INF;
     if (tid == 0) {
         sh.marks = 0; sh.any = 0; sh.wide = 0; sh.iters = 0; sh.tmin = ~0ull; sh.wmax = 0;
-        // which halo sides changed since the last visit; taken before the halo is read, so a neighbour that
-        // marks us afterwards has also queued us for the next round with the bit still set
+        sh.wcnt = 0; sh.wsum = 0;
+        for (int b = 0; b < 8; ++b) sh.mkey[b] = KEY_NONE;
+        // which halo sides changed since the last visit, and the key that queued the tile; taken before the halo
+        // is read, so a neighbour that marks us afterwards has also queued us for the next round with its key
         sh.sides = atomicExch(S.sides + tile, 0u);
+        sh.kvis = a.ordered ? atomicExch(S.tkey + tile, KEY_NONE) : KEY_NONE;
         __threadfence();   // the halo reads below come after the exchange that saw the neighbours' marks
     }
     __syncthreads();
 
     // ---- stage
     stage_dist<DT>(S, dS, x0, y0);
-    unsigned long long wmax = 0;
+    unsigned long long wmax = 0, wsum = 0;
+    unsigned int wcnt = 0;
     bool wide = false;
     bool fallback = false;   // joint search whose weights do not fit 16 bits in this tile: general relaxation
     if (joint) {
@@ -681,6 +719,7 @@ __device__ void visit_tile(const SolveArgs& a, int s, int tile, int round, unsig
                     if (cf < 1e30f && !(__fmul_rn(__fmul_rn(cf, S.maxfac[l]), 16.0f) < WLIM32)) wide = true;
                     const uint32_t wx = qweight<uint32_t>(cf, S.fac[l][0]), wy = qweight<uint32_t>(cf, S.fac[l][2]);
                     const uint32_t wd = qweight<uint32_t>(cf, S.fac[l][4]);
+                    if (wx < INF32) { wsum += wx; ++wcnt; }
                     const int o = l * WLS + r * CSTR + c0 + e;
                     wS[o] = w16(wx);
                     if (S.K == 3) wS[nl * WLS + o] = w16(wy);
@@ -710,6 +749,10 @@ __device__ void visit_tile(const SolveArgs& a, int s, int tile, int round, unsig
                 const float y = __fmul_rn(__fmul_rn(cf, S.maxfac[l]), 16.0f);
                 if (!(y < Lim<DT>::wlim())) wide = true;
                 else wmax = max(wmax, static_cast<unsigned long long>(qweight<DT>(cf, S.maxfac[l])));
+                if (a.ordered) {
+                    const uint32_t wx = qweight<uint32_t>(cf, S.fac[l][0]);
+                    if (wx < INF32) { wsum += wx; ++wcnt; }
+                }
             }
         }
     }
@@ -718,7 +761,14 @@ __device__ void visit_tile(const SolveArgs& a, int s, int tile, int round, unsig
     save_edges<DT>(S, dS, eS);
     if (wide) atomicOr(&sh.wide, 1u);
     if (wmax) atomicMax(&sh.wmax, wmax);
+    if (a.ordered && wcnt) { atomicAdd(&sh.wcnt, wcnt); atomicAdd(&sh.wsum, wsum); }
     __syncthreads();
+    // the search's weight scale (ordered rounds): the least mean straight-move weight of a well-filled tile, i.e.
+    // what a step through open board costs, whatever the congested or blocked parts cost
+    if (a.ordered && tid == 0 && sh.wcnt >= 128) {
+        const unsigned long long mean = sh.wsum / sh.wcnt;
+        atomicMin(&a.st[s].wscale, mean < KEY_NONE ? unsigned(mean) : KEY_NONE - 1);
+    }
 
     // ---- relax to a local fixed point
     bool requeue = false;
@@ -777,53 +827,69 @@ __device__ void visit_tile(const SolveArgs& a, int s, int tile, int round, unsig
         }
         // an edge cell that improved (to at most the bound) below an adjacent neighbour cell's staged value:
         // that neighbour looks again. bits: 0 L, 1 R, 2 T, 3 B, 4 TL, 5 TR, 6 BL, 7 BR
+        // A warp's 32 consecutive entries are the 32 cells of one side of one layer (the loop bound and NT are
+        // multiples of 32), so the warp reduces its marks, and in ordered rounds their keys, before shared atomics.
         unsigned int marks = 0;
         for (int idx = tid; idx < nl * 4 * TILE; idx += NT) {
             const int l = idx / (4 * TILE), side = (idx / TILE) & 3, k = idx % TILE;
             int r, c;
             edge_rc(side, k, r, c);
             const DT v = dS[l * LS + (r + 1) * DSTR + c + 1];
-            if (!(v < eS[idx]) || static_cast<unsigned long long>(v) > ub) continue;
-            const DT* hb = dS + l * LS;
-            // the three halo cells across this side, and the neighbour tile each belongs to
-            for (int t = -1; t <= 1; ++t) {
-                int hr, hc, bit;
-                if (side == 0 || side == 1) {
-                    hr = r + t; hc = side == 0 ? -1 : TILE;
-                    bit = hr < 0 ? (side == 0 ? 4 : 5) : hr >= TILE ? (side == 0 ? 6 : 7) : side;
-                } else {
-                    hc = c + t; hr = side == 2 ? -1 : TILE;
-                    bit = hc < 0 ? (side == 2 ? 4 : 6) : hc >= TILE ? (side == 2 ? 5 : 7) : side;
+            unsigned int bits = 0;
+            if (v < eS[idx] && static_cast<unsigned long long>(v) <= ub) {
+                const DT* hb = dS + l * LS;
+                // the three halo cells across this side, and the neighbour tile each belongs to
+                for (int t = -1; t <= 1; ++t) {
+                    int hr, hc, bit;
+                    if (side == 0 || side == 1) {
+                        hr = r + t; hc = side == 0 ? -1 : TILE;
+                        bit = hr < 0 ? (side == 0 ? 4 : 5) : hr >= TILE ? (side == 0 ? 6 : 7) : side;
+                    } else {
+                        hc = c + t; hr = side == 2 ? -1 : TILE;
+                        bit = hc < 0 ? (side == 2 ? 4 : 6) : hc >= TILE ? (side == 2 ? 5 : 7) : side;
+                    }
+                    if (v < hb[(hr + 1) * DSTR + hc + 1]) bits |= 1u << bit;
                 }
-                if (v < hb[(hr + 1) * DSTR + hc + 1]) marks |= 1u << bit;
+            }
+            const unsigned int wbits = __reduce_or_sync(0xFFFFFFFFu, bits);
+            marks |= wbits;
+            if (a.ordered && wbits) {
+                const uint32_t key = key_of<DT>(v);
+                for (unsigned int rest = wbits; rest; rest &= rest - 1) {
+                    const int b = __ffs(rest) - 1;
+                    const uint32_t kb = __reduce_min_sync(0xFFFFFFFFu, ((bits >> b) & 1u) ? key : KEY_NONE);
+                    if ((tid & 31) == 0) atomicMin(&sh.mkey[b], kb);
+                }
             }
         }
-        if (marks) atomicOr(&sh.marks, marks);
+        if (marks && (tid & 31) == 0) atomicOr(&sh.marks, marks);
         __threadfence();   // the written distances are visible device-wide before any neighbour is marked
     }
     if (tid == 0) sh.iters = unsigned(iters);
     __syncthreads();
+    // lanes 0-7 of warp 0 queue the marked neighbours, lane 8 the tile itself when its visit stopped early, lane 0
+    // updates the search's bound and counters
     if (tid == 0) {
         SStat& st = a.st[s];
         if (sh.tmin != ~0ull && sh.tmin < ub_now) atomicMin(&st.ub, sh.tmin);
         if (sh.wmax) atomicMax(&st.maxw, sh.wmax);
         if (sh.wide) atomicOr(&st.need_wide, 1u);
-        const unsigned int m = sh.marks;
-        const int DXs[8] = {-1, 1, 0, 0, -1, 1, -1, 1}, DYs[8] = {0, 0, -1, 1, -1, -1, 1, 1};
-        for (int b = 0; b < 8; ++b) {
-            if (!((m >> b) & 1)) continue;
-            const int nx = tx + DXs[b], ny = ty + DYs[b];
-            if (nx < 0 || ny < 0 || nx >= S.ntx || ny >= S.nty) continue;
-            atomicOr(S.sides + ny * S.ntx + nx, opposite_side(b));   // the side of the neighbour facing us
-            enqueue(a, S, s, ny * S.ntx + nx, round + 1);
-        }
-        if (requeue) {
-            atomicOr(S.sides + tile, SIDE_ALL);
-            enqueue(a, S, s, tile, round + 1);
-        }
         atomicAdd(a.visits, 1ull);
         atomicAdd(a.visits + 1, static_cast<unsigned long long>(nl));
         atomicAdd(a.visits + 2, static_cast<unsigned long long>(sh.iters));
+    }
+    if (tid < 8 && ((sh.marks >> tid) & 1u)) {
+        const int b = tid;
+        const int DXs[8] = {-1, 1, 0, 0, -1, 1, -1, 1}, DYs[8] = {0, 0, -1, 1, -1, -1, 1, 1};
+        const int nx = tx + DXs[b], ny = ty + DYs[b];
+        if (nx >= 0 && ny >= 0 && nx < S.ntx && ny < S.nty) {
+            atomicOr(S.sides + ny * S.ntx + nx, opposite_side(b));   // the side of the neighbour facing us
+            queue_tile(a, S, s, ny * S.ntx + nx, round + 1, sh.mkey[b]);
+        }
+    }
+    if (tid == 8 && requeue) {
+        atomicOr(S.sides + tile, SIDE_ALL);
+        queue_tile(a, S, s, tile, round + 1, sh.kvis == KEY_NONE ? 0u : sh.kvis);
     }
     __syncthreads();
 }
@@ -836,16 +902,59 @@ __global__ void __launch_bounds__(NT, MINB) relax_kernel(SolveArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ unsigned int sh_item_hi, sh_item_lo, sh_stop;
     const unsigned int nblocks = gridDim.x;
+    const int tid = threadIdx.x;
     int round = 1;
     for (;; ++round) {
         const int buf = round % 3;
         const unsigned int n = *reinterpret_cast<volatile unsigned int*>(a.ctl + C_CNT + buf);
         const unsigned int cnt = n < a.cap ? n : a.cap;
+        // The items visited this round and where the blocks take them from: the round's list itself, or (ordered
+        // rounds) the visit list that the filter below builds from it.
+        const unsigned long long* items = a.wl + size_t(buf) * a.cap;
+        unsigned int* next = a.ctl + C_NEXT + buf;
+        unsigned int vcnt = cnt;
+        if (a.ordered) {
+            // Filter, all threads of the grid over the round's list. A tile whose key is gone was visited after it
+            // was listed (its improvements with it); one keyed above the search's best target has nothing that
+            // can matter; one keyed above the search's band waits for a later round (listed again, its key and
+            // the next round's least key kept). The rest make the visit list.
+            const int vp = round & 1;
+            if (blockIdx.x == 0 && tid == 0) { a.ctl[C_VCNT + (vp ^ 1)] = 0; a.ctl[C_VNEXT + (vp ^ 1)] = 0; }
+            for (int q = blockIdx.x * NT + tid; q < a.n; q += nblocks * NT) a.st[q].kmin[(round + 2) % 3] = KEY_NONE;
+            unsigned long long deferred = 0, dropped = 0;
+            for (unsigned int k = blockIdx.x * NT + tid; k < cnt; k += nblocks * NT) {
+                const unsigned long long it = __ldcg(items + k);
+                const int s = int(it >> 32), tile = int(it & 0xFFFFFFFFu);
+                const SDev& S = a.S[s];
+                const uint32_t key = __ldcg(S.tkey + tile);
+                if (key == KEY_NONE) continue;
+                const SStat& st = a.st[s];
+                const unsigned long long ub = *reinterpret_cast<const volatile unsigned long long*>(&st.ub);
+                if (key > ub) { ++dropped; continue; }
+                const uint32_t km = *reinterpret_cast<const volatile unsigned int*>(&st.kmin[buf]);
+                const uint32_t ws = *reinterpret_cast<const volatile unsigned int*>(&st.wscale);
+                const unsigned long long thr = ws == KEY_NONE || km == KEY_NONE
+                    ? ~0ull : static_cast<unsigned long long>(km) + static_cast<unsigned long long>(ws) * a.band;
+                if (key > thr) {
+                    queue_tile(a, S, s, tile, round + 1, key);
+                    ++deferred;
+                    continue;
+                }
+                const unsigned int pos = atomicAdd(a.ctl + C_VCNT + vp, 1u);
+                a.vl[pos] = it;
+            }
+            if (deferred) atomicAdd(a.visits + 3, deferred);
+            if (dropped) atomicAdd(a.visits + 4, dropped);
+            grid_barrier(a.ctl, nblocks);
+            items = a.vl;
+            next = a.ctl + C_VNEXT + vp;
+            vcnt = *reinterpret_cast<volatile unsigned int*>(a.ctl + C_VCNT + vp);
+        }
         for (;;) {
-            if (threadIdx.x == 0) {
-                const unsigned int k = atomicAdd(a.ctl + C_NEXT + buf, 1u);
-                if (k < cnt) {
-                    const unsigned long long it = __ldcg(a.wl + size_t(buf) * a.cap + k);   // written last round
+            if (tid == 0) {
+                const unsigned int k = atomicAdd(next, 1u);
+                if (k < vcnt) {
+                    const unsigned long long it = __ldcg(items + k);   // written last round, or by the filter
                     sh_item_hi = unsigned(it >> 32);
                     sh_item_lo = unsigned(it & 0xFFFFFFFFu);
                 } else {
@@ -859,13 +968,13 @@ __global__ void __launch_bounds__(NT, MINB) relax_kernel(SolveArgs a) {
             visit_tile<DT>(a, int(hi), int(lo), round, smem);
         }
         // the list consumed last round is free: clear it for the round after next
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (blockIdx.x == 0 && tid == 0) {
             const int fb = (round + 2) % 3;
             a.ctl[C_CNT + fb] = 0;
             a.ctl[C_NEXT + fb] = 0;
         }
         grid_barrier(a.ctl, nblocks);
-        if (threadIdx.x == 0) {
+        if (tid == 0) {
             const unsigned int err = *reinterpret_cast<volatile unsigned int*>(a.ctl + C_ERR);
             const unsigned int nn = *reinterpret_cast<volatile unsigned int*>(a.ctl + C_CNT + (round + 1) % 3);
             sh_stop = (err != 0 || nn == 0) ? 1u : 0u;
@@ -877,7 +986,7 @@ __global__ void __launch_bounds__(NT, MINB) relax_kernel(SolveArgs a) {
         __syncthreads();
         if (sh_stop) break;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) a.ctl[C_ROUNDS] = unsigned(round);
+    if (blockIdx.x == 0 && tid == 0) a.ctl[C_ROUNDS] = unsigned(round);
 }
 
 // starts: distance init (least per state) and the first round's tiles. A start's value is written here, not by a
@@ -902,7 +1011,7 @@ __global__ void seed_kernel(SolveArgs a, const uint32_t* const* sidx, const uint
                 const int nx = tx + dx, ny = ty + dy;
                 if (nx >= 0 && ny >= 0 && nx < S.ntx && ny < S.nty) {
                     atomicOr(S.sides + ny * S.ntx + nx, SIDE_ALL);
-                    enqueue(a, S, s, ny * S.ntx + nx, 1);
+                    queue_tile(a, S, s, ny * S.ntx + nx, 1, key_of<DT>(DT(v)));
                 }
             }
     }
@@ -920,23 +1029,28 @@ __global__ void report_kernel(const SDev* Sv, SStat* stv) {
     const bool have = ub < static_cast<unsigned long long>(INF);
     const size_t RN = size_t(S.rw) * S.rh, N = RN * S.nl;
     unsigned long long bidx = ~0ull, maxd = 0;
+    unsigned int low = 0;
     for (size_t q = size_t(blockIdx.x) * blockDim.x + threadIdx.x; q < N; q += size_t(gridDim.x) * blockDim.x) {
         const int l = int(q / RN), rem = int(q % RN), j = rem / S.rw, i = rem % S.rw;
         const size_t p = (size_t(l) * S.hpad + j) * S.pitch + i;
         const DT d = dist[p];
+        const bool rep = d < INF && (!have || static_cast<unsigned long long>(d) <= ub);
         if (d < INF) {
             maxd = max(maxd, static_cast<unsigned long long>(d));
             if (have && (S.fl[p] & 2) && static_cast<unsigned long long>(d) == ub) bidx = min(bidx, static_cast<unsigned long long>(q));
         }
-        if (S.out) S.out[q] = (d < INF && (!have || static_cast<unsigned long long>(d) <= ub)) ? __ull2float_rn(d) * 0.0625f : 1e30f;
+        low += rep ? 1u : 0u;
+        if (S.out) S.out[q] = rep ? __ull2float_rn(d) * 0.0625f : 1e30f;
     }
     for (int o = 16; o; o >>= 1) {
         bidx = min(bidx, __shfl_xor_sync(0xFFFFFFFFu, bidx, o));
         maxd = max(maxd, __shfl_xor_sync(0xFFFFFFFFu, maxd, o));
+        low += __shfl_xor_sync(0xFFFFFFFFu, low, o);
     }
     if ((threadIdx.x & 31) == 0) {
         if (bidx != ~0ull) atomicMin(&st.best, bidx);
         if (maxd) atomicMax(&st.maxd, maxd);
+        if (low) atomicAdd(&st.settled, low);
     }
 }
 
@@ -1018,8 +1132,20 @@ struct DevBuf {
 };
 
 struct Arena {
-    DevBuf dist, stamp, wl, sdev, sstat, ctl, visits, sptr;
+    DevBuf dist, stamp, tkey, wl, vl, sdev, sstat, ctl, visits, sptr;
 } g_arena;
+
+// Band of an ordered round, in multiples of a search's weight scale (the cost of one step through open board);
+// 0 runs every queued tile each round. Set by pcbg_set_round_band or the autotuner.
+int g_band = 16;
+// Round cap of a launch: a bound on the device loop, which tests lower (pcbg_set_max_rounds, or PCBG_MAX_ROUNDS in
+// the environment of a process such as the router) to see a launch stop with ERR_ROUNDS and its caller fall back.
+int max_rounds_from_env() {
+    const char* e = std::getenv("PCBG_MAX_ROUNDS");
+    const int v = e ? std::atoi(e) : 0;
+    return v >= 1 ? v : (1 << 20);
+}
+int g_max_rounds = max_rounds_from_env();
 
 thread_local std::string t_err;
 thread_local BatchStats t_stats;
@@ -1086,8 +1212,13 @@ void classify(SDev& S) {
 }
 
 // Solve items[idx[0..m)] with DT distances.
+void init_stat(SStat& x) {
+    x.ub = ~0ull; x.maxw = 0; x.best = ~0ull; x.maxd = 0; x.need_wide = 0;
+    x.wscale = KEY_NONE; x.kmin[0] = x.kmin[1] = x.kmin[2] = KEY_NONE; x.settled = 0;
+}
+
 template <typename DT>
-int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream, BatchStats& bs) {
+int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream, BatchStats& bs, int band) {
     const int m = int(idx.size());
     std::vector<SDev> sd(m);
     std::vector<size_t> doff(m), toff(m);
@@ -1123,9 +1254,10 @@ int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream
     if (any_general) smem = std::max(smem, layout(nlmax, 4, sizeof(DT)).total);
     Arena& A = g_arena;
     const unsigned int cap = unsigned(std::max<size_t>(tiles, 1));
-    if (!A.dist.need(dbytes) || !A.stamp.need(tiles * 8 + 8) || !A.wl.need(size_t(3) * cap * 8) ||
+    if (!A.dist.need(dbytes) || !A.stamp.need(tiles * 8 + 8) || !A.tkey.need(tiles * 4 + 4) ||
+        !A.wl.need(size_t(3) * cap * 8) || !A.vl.need(size_t(cap) * 8) ||
         !A.sdev.need(sizeof(SDev) * m) || !A.sstat.need(sizeof(SStat) * m) || !A.ctl.need(C_N * 4) ||
-        !A.visits.need(24) || !A.sptr.need(size_t(m) * (8 + 8 + 4) + 64)) {
+        !A.visits.need(NVIS * 8) || !A.sptr.need(size_t(m) * (8 + 8 + 4) + 64)) {
         t_err = "device allocation failed";
         return -1;
     }
@@ -1133,18 +1265,19 @@ int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream
         sd[k].dist = static_cast<unsigned char*>(A.dist.p) + doff[k];
         sd[k].stamp = static_cast<uint32_t*>(A.stamp.p) + toff[k];
         sd[k].sides = static_cast<uint32_t*>(A.stamp.p) + tiles + toff[k];
+        sd[k].tkey = static_cast<uint32_t*>(A.tkey.p) + toff[k];
     }
     // the batch's descriptors, initial stats and start lists go up from pinned staging (asynchronous copies; a copy
     // from pageable memory would go through the driver's bounce buffer one call at a time)
     const size_t h_sd = 0, h_st = round_up(sizeof(SDev) * m, 16), h_sp = h_st + round_up(sizeof(SStat) * m, 16);
     const size_t h_res = h_sp + round_up(size_t(m) * 20, 16), h_ctl = h_res + round_up(sizeof(SStat) * m, 16);
-    const size_t h_vis = h_ctl + 64, h_end = h_vis + 32;
+    const size_t h_vis = h_ctl + 64, h_end = h_vis + NVIS * 8;
     if (!host_stage(h_end)) { t_err = "pinned allocation failed"; return -1; }
     unsigned char* hs = g_hstage.p;
     memcpy(hs + h_sd, sd.data(), sizeof(SDev) * m);
     SStat* st0 = reinterpret_cast<SStat*>(hs + h_st);
     for (int k = 0; k < m; ++k) {
-        st0[k].ub = ~0ull; st0[k].maxw = 0; st0[k].best = ~0ull; st0[k].maxd = 0; st0[k].need_wide = 0; st0[k].pad = 0;
+        init_stat(st0[k]);
         reinterpret_cast<const uint32_t**>(hs + h_sp)[k] = items[idx[k]].start_idx;
         reinterpret_cast<const uint64_t**>(hs + h_sp + size_t(m) * 8)[k] = items[idx[k]].start_d;
         reinterpret_cast<int*>(hs + h_sp + size_t(m) * 16)[k] = items[idx[k]].n_starts;
@@ -1158,8 +1291,9 @@ int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream
     cudaMemcpyAsync(sp, hs + h_sp, size_t(m) * 20, cudaMemcpyHostToDevice, stream);
     cudaMemsetAsync(A.dist.p, 0x7F, dbytes, stream);
     cudaMemsetAsync(A.stamp.p, 0, tiles * 8 + 8, stream);
+    cudaMemsetAsync(A.tkey.p, 0xFF, tiles * 4 + 4, stream);
     cudaMemsetAsync(A.ctl.p, 0, C_N * 4, stream);
-    cudaMemsetAsync(A.visits.p, 0, 24, stream);
+    cudaMemsetAsync(A.visits.p, 0, NVIS * 8, stream);
     SolveArgs a;
     a.S = static_cast<const SDev*>(A.sdev.p);
     a.st = static_cast<SStat*>(A.sstat.p);
@@ -1167,10 +1301,13 @@ int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream
     a.nlmax = nlmax;
     a.kmax = kmax;
     a.wl = static_cast<unsigned long long*>(A.wl.p);
+    a.vl = static_cast<unsigned long long*>(A.vl.p);
     a.cap = cap;
     a.ctl = static_cast<unsigned int*>(A.ctl.p);
     a.visits = static_cast<unsigned long long*>(A.visits.p);
-    a.max_rounds = 1 << 20;
+    a.max_rounds = g_max_rounds;
+    a.band = unsigned(band);
+    a.ordered = sizeof(DT) == 4 && band > 0 ? 1 : 0;
     seed_kernel<DT><<<m, 128, 0, stream>>>(a, d_sip, d_sdp, d_ns);
     const RelaxLaunch R = relax_launch<DT>(smem, tiles);
     if (R.resident <= 0) { t_err = "relax kernel cannot be resident"; return -1; }
@@ -1193,7 +1330,7 @@ int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream
     const unsigned long long* visits = reinterpret_cast<const unsigned long long*>(hs + h_vis);
     cudaMemcpyAsync(hs + h_res, A.sstat.p, sizeof(SStat) * m, cudaMemcpyDeviceToHost, stream);
     cudaMemcpyAsync(hs + h_ctl, A.ctl.p, C_N * 4, cudaMemcpyDeviceToHost, stream);
-    cudaMemcpyAsync(hs + h_vis, A.visits.p, 24, cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(hs + h_vis, A.visits.p, NVIS * 8, cudaMemcpyDeviceToHost, stream);
     e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) { t_err = std::string("batch solve: ") + cudaGetErrorString(e); return -1; }
     if (ctl[C_ERR]) {
@@ -1207,6 +1344,8 @@ int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream
     bs.tile_visits += (long long)visits[0];
     bs.layer_visits += (long long)visits[1];
     bs.local_iters += (long long)visits[2];
+    bs.deferred += (long long)visits[3];
+    bs.dropped += (long long)visits[4];
     const int rounds_out = int(ctl[C_ROUNDS]);
     const unsigned long long INF = static_cast<unsigned long long>(Lim<DT>::INF);
     for (int k = 0; k < m; ++k) {
@@ -1223,6 +1362,7 @@ int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream
             if (!have && x.maxd + x.maxw >= INF) redo = true;
         }
         b.status = redo ? 1 : 0;
+        if (!redo) bs.settled += x.settled;
     }
     return 0;
 }
@@ -1247,12 +1387,12 @@ int solve_batch(BatchItem* items, int n, cudaStream_t stream) {
     }
     std::vector<int> all(n);
     for (int k = 0; k < n; ++k) all[k] = k;
-    if (run_batch<uint32_t>(items, all, stream, t_stats) != 0) return -1;
+    if (run_batch<uint32_t>(items, all, stream, t_stats, g_band) != 0) return -1;
     std::vector<int> wide;
     for (int k = 0; k < n; ++k)
         if (items[k].status == 1) wide.push_back(k);
     if (!wide.empty()) {
-        if (run_batch<uint64_t>(items, wide, stream, t_stats) != 0) return -1;
+        if (run_batch<uint64_t>(items, wide, stream, t_stats, 0) != 0) return -1;
         for (int k : wide) items[k].status = 1;
     }
     return 0;
@@ -1291,32 +1431,53 @@ extern "C" int64_t pcbg_last_batch_layer_visits(void) { return pcbg::last_stats(
 extern "C" float pcbg_last_batch_kernel_ms(void) { return pcbg::last_stats().kernel_ms; }
 extern "C" int32_t pcbg_last_batch_launches(void) { return pcbg::last_stats().launches; }
 extern "C" int64_t pcbg_last_batch_local_iters(void) { return pcbg::last_stats().local_iters; }
+extern "C" int64_t pcbg_last_batch_deferred(void) { return pcbg::last_stats().deferred; }
+extern "C" int64_t pcbg_last_batch_dropped(void) { return pcbg::last_stats().dropped; }
+extern "C" int64_t pcbg_last_batch_settled(void) { return pcbg::last_stats().settled; }
+
+extern "C" void pcbg_set_round_band(int32_t band) {
+    std::lock_guard<std::mutex> g(pcbg::g_mu);
+    pcbg::g_band = band < 0 ? 0 : band;
+}
+extern "C" int32_t pcbg_round_band(void) { return pcbg::g_band; }
+
+extern "C" void pcbg_set_max_rounds(int32_t rounds) {
+    std::lock_guard<std::mutex> g(pcbg::g_mu);
+    pcbg::g_max_rounds = rounds < 1 ? (1 << 20) : rounds;
+}
 
 // ---- pcbg_solve_noalloc: one search with all scratch in a static device array ----
 //
 // For callers that cannot allocate device memory. Everything the batch path takes from its grow-only arena
-// (distances, tile stamps, worklists, descriptors, control words) is carved here from one file-scope array of fixed
-// size instead, and the host side uses only stack storage.
+// (distances, tile stamps, keys, worklists, descriptors, control words) is carved here from one file-scope array of
+// fixed size instead, and the host side uses only stack storage.
 
 static __device__ __align__(256) unsigned char pcbg_noalloc_scratch[
-    PCBG_NOALLOC_MAX_STATES * 8 +                                          // distances, room for 64-bit
-    (PCBG_NOALLOC_MAX_STATES / (pcbg::TILE * pcbg::TILE)) * (8 + 3 * 8) +  // tile stamps + sides, 3 worklists
-    4096];                                                                  // descriptors, control words
+    PCBG_NOALLOC_MAX_STATES * 8 +                                                  // distances, room for 64-bit
+    (PCBG_NOALLOC_MAX_STATES / (pcbg::TILE * pcbg::TILE)) * (8 + 4 + 3 * 8 + 8) +  // tile stamps + sides, keys,
+                                                                                   // 3 worklists, visit list
+    4096];                                                                          // descriptors, control words
 
 namespace pcbg {
 namespace {
 
 constexpr size_t NA_TILES = PCBG_NOALLOC_MAX_STATES / (TILE * TILE);
 constexpr size_t NA_DIST = size_t(PCBG_NOALLOC_MAX_STATES) * 8;
-constexpr size_t NA_STAMP = NA_TILES * 8;   // stamps, then sides
-constexpr size_t NA_WL = NA_TILES * 3 * 8;
-// offsets in the small area after the worklists
-constexpr size_t NA_SDEV = 0, NA_SSTAT = 1024, NA_CTL = 1088, NA_VIS = 1152, NA_SPTR = 1184;
+constexpr size_t NA_STAMP = NA_DIST;                       // stamps, then sides
+constexpr size_t NA_TKEY = NA_STAMP + NA_TILES * 8;
+constexpr size_t NA_WL = NA_TKEY + NA_TILES * 4;
+constexpr size_t NA_VL = NA_WL + NA_TILES * 3 * 8;
+constexpr size_t NA_SMALL = NA_VL + NA_TILES * 8;
+// offsets in the small area after the lists
+constexpr size_t NA_SDEV = 0, NA_SSTAT = 1024, NA_CTL = 1088, NA_VIS = 1152, NA_SPTR = 1216;
+static_assert(sizeof(SDev) <= NA_SSTAT - NA_SDEV && sizeof(SStat) <= NA_CTL - NA_SSTAT &&
+              C_N * 4 <= NA_VIS - NA_CTL && NVIS * 8 <= NA_SPTR - NA_VIS && NA_SPTR + 24 <= 4096,
+              "no-alloc small area layout");
+static_assert(NA_SMALL + 4096 == sizeof(pcbg_noalloc_scratch), "no-alloc scratch layout");
 
 std::mutex g_na_mu;
 void* g_na_base[64] = {};
 
-// device address of the static scratch on the current device (looked up once per device)
 // error text without heap allocation: the thread's message buffer is reserved during set-up
 void na_error(const char* fmt, const char* a = "", long long x = 0, long long y = 0) {
     char buf[200];
@@ -1324,6 +1485,7 @@ void na_error(const char* fmt, const char* a = "", long long x = 0, long long y 
     t_err.assign(buf);
 }
 
+// device address of the static scratch on the current device (looked up once per device)
 unsigned char* na_base() {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) { na_error("no current device%s"); return nullptr; }
@@ -1338,7 +1500,7 @@ unsigned char* na_base() {
 }
 
 template <typename DT>
-int na_run(pcbg_search* q, unsigned char* base, cudaStream_t stream) {
+int na_run(pcbg_search* q, unsigned char* base, cudaStream_t stream, int band) {
     SDev S;
     memset(&S, 0, sizeof(S));
     S.rw = q->rw; S.rh = q->rh; S.nl = q->nl; S.pitch = q->pitch; S.hpad = q->hpad;
@@ -1351,47 +1513,62 @@ int na_run(pcbg_search* q, unsigned char* base, cudaStream_t stream) {
     classify(S);
     if (sizeof(DT) != 4) S.mode = 0;
     S.cf = q->cf; S.fl = q->flags; S.vcf = q->vcf; S.out = q->out;
+    S.path = q->path; S.path_len = q->path_len; S.path_cap = q->path_cap;
     const size_t states = size_t(q->nl) * q->hpad * q->pitch, tiles = size_t(S.ntx) * S.nty;
-    unsigned char* small = base + NA_DIST + NA_STAMP + NA_WL;
+    // the launch shape first: nothing is queued on the stream unless the relaxation can be launched
+    const size_t smem = S.mode ? layout(q->nl, joint_wbytes(S.K), 4).total : layout(q->nl, 4, sizeof(DT)).total;
+    const RelaxLaunch R = relax_launch<DT>(smem, tiles);
+    if (R.resident <= 0) { na_error("relax kernel cannot be resident%s"); return -1; }
+    // a round visits each queued tile once: more blocks than tiles would only wait at the grid barriers
+    const int blocks = int(std::min<size_t>(size_t(R.resident), std::max<size_t>(tiles, 1)));
+    unsigned char* small = base + NA_SMALL;
     S.dist = base;
-    S.stamp = reinterpret_cast<uint32_t*>(base + NA_DIST);
+    S.stamp = reinterpret_cast<uint32_t*>(base + NA_STAMP);
     S.sides = S.stamp + NA_TILES;
+    S.tkey = reinterpret_cast<uint32_t*>(base + NA_TKEY);
     SStat st0;
-    st0.ub = ~0ull; st0.maxw = 0; st0.best = ~0ull; st0.maxd = 0; st0.need_wide = 0; st0.pad = 0;
+    init_stat(st0);
     const void* sptr[2] = {q->start_idx, q->start_d};
     const int ns = q->n_starts;
     cudaMemcpyAsync(small + NA_SDEV, &S, sizeof(S), cudaMemcpyHostToDevice, stream);
     cudaMemcpyAsync(small + NA_SSTAT, &st0, sizeof(st0), cudaMemcpyHostToDevice, stream);
     cudaMemcpyAsync(small + NA_SPTR, sptr, sizeof(sptr), cudaMemcpyHostToDevice, stream);
     cudaMemcpyAsync(small + NA_SPTR + 16, &ns, sizeof(ns), cudaMemcpyHostToDevice, stream);
-    // the array keeps the previous call's contents: clear what must start unreached / zero
+    // the array keeps the previous call's contents: clear what must start unreached / zero / keyless
     cudaMemsetAsync(base, 0x7F, states * sizeof(DT), stream);
-    cudaMemsetAsync(base + NA_DIST, 0, tiles * 4, stream);
-    cudaMemsetAsync(base + NA_DIST + NA_TILES * 4, 0, tiles * 4, stream);
+    cudaMemsetAsync(base + NA_STAMP, 0, tiles * 4, stream);
+    cudaMemsetAsync(base + NA_STAMP + NA_TILES * 4, 0, tiles * 4, stream);
+    cudaMemsetAsync(base + NA_TKEY, 0xFF, tiles * 4, stream);
     cudaMemsetAsync(small + NA_CTL, 0, C_N * 4, stream);
-    cudaMemsetAsync(small + NA_VIS, 0, 24, stream);
+    cudaMemsetAsync(small + NA_VIS, 0, NVIS * 8, stream);
     SolveArgs a;
     a.S = reinterpret_cast<const SDev*>(small + NA_SDEV);
     a.st = reinterpret_cast<SStat*>(small + NA_SSTAT);
     a.n = 1;
     a.nlmax = q->nl;
     a.kmax = S.mode ? S.K : 0;
-    a.wl = reinterpret_cast<unsigned long long*>(base + NA_DIST + NA_STAMP);
+    a.wl = reinterpret_cast<unsigned long long*>(base + NA_WL);
+    a.vl = reinterpret_cast<unsigned long long*>(base + NA_VL);
     a.cap = unsigned(tiles);
     a.ctl = reinterpret_cast<unsigned int*>(small + NA_CTL);
     a.visits = reinterpret_cast<unsigned long long*>(small + NA_VIS);
-    a.max_rounds = 1 << 20;
-    seed_kernel<DT><<<1, 128, 0, stream>>>(a, reinterpret_cast<const uint32_t* const*>(small + NA_SPTR),
-                                          reinterpret_cast<const uint64_t* const*>(small + NA_SPTR + 8),
-                                          reinterpret_cast<const int*>(small + NA_SPTR + 16));
-    const size_t smem = S.mode ? layout(q->nl, joint_wbytes(S.K), 4).total : layout(q->nl, 4, sizeof(DT)).total;
-    const RelaxLaunch R = relax_launch<DT>(smem, tiles);
-    const int blocks = R.resident;
-    if (blocks <= 0) { na_error("relax kernel cannot be resident%s"); return -1; }
+    a.max_rounds = g_max_rounds;
+    a.band = unsigned(band);
+    a.ordered = sizeof(DT) == 4 && band > 0 ? 1 : 0;
+    const uint32_t* const* sip = reinterpret_cast<const uint32_t* const*>(small + NA_SPTR);
+    const uint64_t* const* sdp = reinterpret_cast<const uint64_t* const*>(small + NA_SPTR + 8);
+    const int* nsp = reinterpret_cast<const int*>(small + NA_SPTR + 16);
+    seed_kernel<DT><<<1, 128, 0, stream>>>(a, sip, sdp, nsp);
     void* args[] = {&a};
     cudaError_t e = cudaLaunchCooperativeKernel(R.fn, dim3(blocks), dim3(NT), args, smem, stream);
-    if (e != cudaSuccess) { na_error("cooperative launch: %s", cudaGetErrorString(e)); return -1; }
+    if (e != cudaSuccess) {
+        // the copies, clears and seeds queued above must be done before another call can reuse the array
+        cudaStreamSynchronize(stream);
+        na_error("cooperative launch: %s", cudaGetErrorString(e));
+        return -1;
+    }
     report_kernel<DT><<<dim3(32, 1), 256, 0, stream>>>(a.S, a.st);
+    if (q->path) walkback_kernel<DT><<<1, 32, 0, stream>>>(a.S, a.st, sip, sdp, nsp);
     SStat x;
     unsigned int ctl[C_N];
     cudaMemcpyAsync(&x, small + NA_SSTAT, sizeof(x), cudaMemcpyDeviceToHost, stream);
@@ -1434,9 +1611,9 @@ extern "C" int pcbg_solve_noalloc(pcbg_search* s, void* stream) {
     if (!base) return PCBG_ERR_FAIL;
     std::lock_guard<std::mutex> g(g_mu);  // one solve at a time in this process: calls share the array
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    if (na_run<uint32_t>(s, base, st) != 0) return PCBG_ERR_FAIL;
+    if (na_run<uint32_t>(s, base, st, g_band) != 0) return PCBG_ERR_FAIL;
     if (s->status == 1) {
-        if (na_run<uint64_t>(s, base, st) != 0) return PCBG_ERR_FAIL;
+        if (na_run<uint64_t>(s, base, st, 0) != 0) return PCBG_ERR_FAIL;
         s->status = 1;
     }
     return 0;

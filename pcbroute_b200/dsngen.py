@@ -6,7 +6,12 @@ Boards are deterministic functions of (config, seed). Footprints are built from 
 - QFP-100: 25 pads per side, 0.3 x 1.5 mm, 0.5 mm pitch, 15.4 mm across the pad rows;
 - BGA-256: 16 x 16 balls of 0.5 mm, 1.0 mm pitch.
 Vias are through-hole (one circle per copper layer). Parts are placed at random without overlapping (with a
-courtyard margin); nets take random pins; classes and planes follow the configuration.
+courtyard margin), or, on boards whose courtyards fill more than 40 % of the area, packed in rows of shuffled parts
+with the slack of each row spread at random; nets take random pins; classes and planes follow the configuration.
+
+A board needs nets + connections pins (a net of k pins makes k - 1 connections). Where the parts a configuration
+names carry fewer pins than its nets and connections need, pin-bearing parts (QFP-100s, SOIC-8s) are added, and
+the counts below say so.
 
     python -m pcbroute_b200.dsngen c1 1 board.dsn
 """
@@ -94,22 +99,25 @@ class Config:
 
 
 CONFIGS = {
-    # 2 layers, 12 parts (SOIC-8 / 0805), 40 nets, ~60 two-pin connections, one class 250/200 um
-    "c1": Config("c1", 50, 40, ["F.Cu", "B.Cu"], [("SOIC8", 10), ("R0805", 2)], 40, 60),
-    # 4 layers with GND / VCC planes, QFP-100 + 40 0402/0603, 300 nets, 500 connections, 20 % multi-pin (2-6)
+    # 2 layers, 12 SOIC-8 (96 pins), 40 nets, one class 250/200 um. 60 connections over 40 nets would need 100 pins:
+    # 96 make 40 nets of 56 connections (multi-pin nets of 3 pins).
+    "c1": Config("c1", 50, 40, ["F.Cu", "B.Cu"], [("SOIC8", 12)], 40, 56, 0.4, (3, 3)),
+    # 4 layers with GND / VCC planes, QFP-100 + 40 0402/0603, 300 nets / 500 connections (800 pins and the planes':
+    # 80 SOIC-8 added), 20 % multi-pin (3-6), two classes
     "c2": Config("c2", 100, 80, ["F.Cu", "In1.Cu", "In2.Cu", "B.Cu"],
-                 [("QFP100", 1), ("R0402", 20), ("R0603", 20), ("SOIC8", 12)], 300, 500, 0.2, (3, 6),
+                 [("QFP100", 1), ("R0402", 20), ("R0603", 20), ("SOIC8", 80)], 300, 500, 0.2, (3, 6),
                  [("default", 200, 150, 0.85), ("power", 400, 250, 0.15)], [("GND", "In1.Cu"), ("VCC", "In2.Cu")]),
-    # 6 layers, BGA-256 at 1.0 mm pitch + 150 passives (+ SOIC-8s for pins), up to 1200 nets / 2000 connections as
-    # the pins allow, 20 % multi-pin (3-6), two classes
+    # 6 layers, a BGA-256 at 1.0 mm pitch + 150 passives, 1200 nets / 2000 connections (3200 pins: 24 QFP-100 and
+    # 40 SOIC-8 added), 20 % multi-pin (3-6), two classes
     "c4": Config("c4", 160, 100, ["F.Cu", "In1.Cu", "In2.Cu", "In3.Cu", "In4.Cu", "B.Cu"],
-                 [("BGA256", 2), ("R0402", 75), ("R0603", 75), ("SOIC8", 120)], 1200, 2000, 0.2, (3, 6),
-                 [("default", 200, 150, 0.85), ("power", 400, 250, 0.15)]),
-    # 8 layers, 250 x 200 mm, up to 3000 nets / 6000 connections as the pins allow, four classes
+                 [("BGA256", 1), ("QFP100", 24), ("SOIC8", 40), ("R0402", 75), ("R0603", 75)], 1200, 2000, 0.2,
+                 (3, 6), [("default", 200, 150, 0.85), ("power", 400, 250, 0.15)]),
+    # 8 layers, 250 x 200 mm, 3000 nets / 6000 connections (9000 pins and the planes': 4 BGA-256, 60 QFP-100, 102
+    # SOIC-8 and 600 passives), 30 % multi-pin (3-6), four classes, GND / VCC planes
     "c5": Config("c5", 250, 200, ["F.Cu", "In1.Cu", "In2.Cu", "In3.Cu", "In4.Cu", "In5.Cu", "In6.Cu", "B.Cu"],
-                 [("BGA256", 4), ("R0402", 300), ("R0603", 300), ("SOIC8", 300)], 3000, 6000, 0.3, (3, 6),
-                 [("default", 150, 150, 0.6), ("signal", 200, 150, 0.2), ("power", 400, 250, 0.15),
-                  ("hv", 500, 400, 0.05)], [("GND", "In1.Cu"), ("VCC", "In6.Cu")]),
+                 [("BGA256", 4), ("QFP100", 60), ("SOIC8", 102), ("R0402", 300), ("R0603", 300)], 3000, 6000, 0.3,
+                 (3, 6), [("default", 150, 150, 0.6), ("signal", 200, 150, 0.2), ("power", 400, 250, 0.15),
+                          ("hv", 500, 400, 0.05)], [("GND", "In1.Cu"), ("VCC", "In6.Cu")]),
     # small boards for the parity tests
     "t1": Config("t1", 24, 18, ["F.Cu", "B.Cu"], [("SOIC8", 3), ("R0805", 4)], 10, 14),
     "t2": Config("t2", 30, 24, ["F.Cu", "In1.Cu", "In2.Cu", "B.Cu"], [("SOIC8", 4), ("R0603", 6)], 16, 24, 0.2, (3, 4),
@@ -117,8 +125,53 @@ CONFIGS = {
 }
 
 
+def _pack(rng, cfg):
+    """Rows of shuffled parts, tallest first within the board's width; each row's leftover width is spread at random
+    between its parts, and each part sits at a random height within its row."""
+    W, H = cfg.w_mm * 1000, cfg.h_mm * 1000
+    inst = []
+    for fp_name, count in cfg.parts:
+        fp = FOOTPRINTS[fp_name]
+        for _ in range(count):
+            rot = rng.choice([0, 90]) if fp.w != fp.h else 0
+            w, h = (fp.w, fp.h) if rot == 0 else (fp.h, fp.w)
+            inst.append((fp_name, w, h, rot))
+    rng.shuffle(inst)
+    inst.sort(key=lambda t: -t[2])
+    gap, edge = 600, 1500
+    rows, row, x = [], [], edge
+    for it in inst:
+        if row and x + it[1] > W - edge:
+            rows.append(row)
+            row, x = [], edge
+        row.append(it)
+        x += it[1] + gap
+    if row:
+        rows.append(row)
+    placed, y = [], edge
+    for row in rows:
+        rh = max(it[2] for it in row)
+        if y + rh > H - edge:
+            break                                  # the board is full: the parts left over are not placed
+        slack = (W - 2 * edge) - sum(it[1] for it in row) - gap * (len(row) - 1)
+        cuts = sorted(rng.uniform(0, max(0.0, slack)) for _ in range(len(row)))
+        x, prev = edge, 0.0
+        for it, c in zip(row, cuts):
+            x += c - prev
+            prev = c
+            fp_name, w, h, rot = it
+            yy = y + rng.uniform(0, rh - h)
+            placed.append((fp_name, f"{fp_name[0]}{len(placed) + 1}", round(x + w / 2), round(yy + h / 2), w, h, rot))
+            x += w + gap
+        y += rh + gap
+    return placed
+
+
 def _place(rng, cfg):
     W, H = cfg.w_mm * 1000, cfg.h_mm * 1000
+    area = sum((FOOTPRINTS[f].w + 600) * (FOOTPRINTS[f].h + 600) * n for f, n in cfg.parts)
+    if area > 0.4 * (W - 3000) * (H - 3000):
+        return _pack(rng, cfg)
     placed = []
     for fp_name, count in cfg.parts:
         fp = FOOTPRINTS[fp_name]
@@ -146,17 +199,25 @@ def generate(config: str, seed: int) -> str:
     for net, _layer in cfg.planes:
         k = min(len(pins), rng.randint(4, 8))
         nets.append((net, [pins.pop() for _ in range(k)]))
-    conns = 0
-    i = 0
-    while len(nets) < cfg.nets + len(cfg.planes) and len(pins) >= 2 and conns < cfg.connections:
-        multi = rng.random() < cfg.multipin_frac
-        k = rng.randint(*cfg.fanout) if multi else 2
-        k = min(k, len(pins), cfg.connections - conns + 1)
-        if k < 2:
-            break
+    # net sizes: the configured share of multi-pin nets start at the fan-out's low end, then the connections still
+    # missing go one pin at a time to random multi-pin nets below the fan-out's high end
+    sizes = [2] * cfg.nets
+    multi = rng.sample(range(cfg.nets), round(cfg.multipin_frac * cfg.nets))
+    for m in multi:
+        sizes[m] = cfg.fanout[0]
+    extra = cfg.connections - sum(k - 1 for k in sizes)
+    open_ = [m for m in multi if sizes[m] < cfg.fanout[1]]
+    while extra > 0 and open_:
+        m = rng.choice(open_)
+        sizes[m] += 1
+        extra -= 1
+        if sizes[m] >= cfg.fanout[1]:
+            open_.remove(m)
+    for i, k in enumerate(sizes):
+        if len(pins) < 2:
+            break                                 # out of pins: the board holds fewer nets
+        k = min(k, len(pins))
         nets.append((f"N{i}", [pins.pop() for _ in range(k)]))
-        conns += k - 1
-        i += 1
     # classes: a share of the signal nets each
     names = [n for n, _ in nets]
     cls_of = {}

@@ -92,6 +92,47 @@ class Scheduler:
             pass
 
 
+def read_router_log(path: str) -> tuple[np.ndarray, np.ndarray]:
+    """The labelled pairs a router wrote in log mode (PCBG_SCHED=log, include/pcbg.h): records of an int64 row count,
+    rows x FEATURES bf16 bit patterns and rows u8 labels. Returns (x [n, FEATURES] uint16, y [n] float32)."""
+    xs, ys = [], []
+    with open(path, "rb") as f:
+        while True:
+            h = f.read(8)
+            if len(h) < 8:
+                break
+            n = int(np.frombuffer(h, np.int64)[0])
+            x = np.frombuffer(f.read(n * FEATURES * 2), np.uint16).reshape(n, FEATURES)
+            y = np.frombuffer(f.read(n), np.uint8).astype(np.float32)
+            xs.append(x)
+            ys.append(y)
+    if not xs:
+        return np.zeros((0, FEATURES), np.uint16), np.zeros(0, np.float32)
+    return np.concatenate(xs), np.concatenate(ys)
+
+
+def train_router_model(log_paths: list[str], out_path: str, epochs: int = 12, lr: float = 1e-3, batch: int = 256,
+                       seed: int = 1) -> dict:
+    """Fit the conflict predictor on the GPU (the library's own forward / backward kernels and Adam) to the pairs
+    routers logged, and write its parameters (float32, pcbg_sched_get_params order) to out_path for
+    PCBG_SCHED_MODEL."""
+    import time
+    xs, ys = zip(*(read_router_log(p) for p in log_paths))
+    x = np.ascontiguousarray(np.concatenate(xs))
+    y = np.ascontiguousarray(np.concatenate(ys))
+    sch = Scheduler(seed)
+    if sch.lib.pcbg_sched_add_log_host(sch.h, x.ctypes.data, y.ctypes.data, len(y)) != 0:
+        raise RuntimeError(_lib.last_error())
+    loss = C.c_float(0)
+    t0 = time.perf_counter()
+    if sch.lib.pcbg_sched_train(sch.h, epochs, C.c_float(lr), batch, seed, C.byref(loss)) != 0:
+        raise RuntimeError(_lib.last_error())
+    secs = time.perf_counter() - t0
+    sch.params().tofile(out_path)
+    return {"pairs": int(len(y)), "positives": int(y.sum()), "epochs": epochs, "loss": float(loss.value),
+            "train_s": round(secs, 3)}
+
+
 def collect_logs(sch: Scheduler, boards: list[dict], iters: int, width: int) -> None:
     """Conflict logs of plain speculative rounds: every board negotiated `iters` iterations, pairs labelled after
     each iteration."""

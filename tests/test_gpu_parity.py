@@ -136,6 +136,73 @@ def test_large_batch_matches_oracle(gpu):
         assert np.array_equal(got.view(np.uint32), field.view(np.uint32)), k
 
 
+def _oracle_many(searches, threads=None):
+    """oracle_of over many searches on host threads (the C oracle releases the GIL)."""
+    import os
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(threads or os.cpu_count() or 1) as ex:
+        return list(ex.map(oracle_of, searches))
+
+
+def _check_fields(searches, arr, refs, tag):
+    for k, (s, (field, best, bd)) in enumerate(zip(searches, refs)):
+        assert arr[k].best == best, (tag, k, arr[k].best, best)
+        if best >= 0:
+            assert arr[k].best_d == bd, (tag, k)
+        got = s["out"].cpu().numpy().reshape(s["nl"], s["rh"], s["rw"])
+        assert np.array_equal(got.view(np.uint32), field.view(np.uint32)), (tag, k)
+        del s["out"]
+
+
+def test_largest_microbenchmark_searches_match_oracle(gpu):
+    """The 8 largest searches of the benchmarked workload (windows up to 2047 x 2047 with up to 6 layers, 32-bit
+    distances near their largest values) in one launch, large enough for the 3-blocks-per-SM build: fields, best
+    targets and their costs equal the oracle's bit for bit."""
+    sizes = synth.microbench_sizes(20261203, 4096)
+    big = sorted(range(len(sizes)), key=lambda k: -sizes[k][0] * sizes[k][1] * sizes[k][2])[:8]
+    assert max(sizes[k][0] for k in big) >= 1800 and max(sizes[k][2] for k in big) == 6
+    searches = [make_device_search(sizes[k][4], sizes[k][0], sizes[k][1], sizes[k][2], sizes[k][3]) for k in big]
+    arr = run_batch(searches)
+    refs = _oracle_many(searches)
+    _check_fields(searches, arr, refs, "largest")
+
+
+def test_eight_layer_searches_match_oracle(gpu):
+    """8-layer windows of 1024 x 1024 and more (the most shared memory per visit) against the oracle."""
+    searches = [make_device_search(9800 + k, rw, rh, 8, via)
+                for k, (rw, rh, via) in enumerate([(1024, 1024, 12.0), (1200, 1100, 30.0)])]
+    arr = run_batch(searches)
+    _check_fields(searches, arr, _oracle_many(searches), "8 layers")
+
+
+@pytest.mark.parametrize("band", [0, 1, 4, 64])
+def test_round_band_changes_work_not_results(gpu, band):
+    """Ordered rounds (pcbg_set_round_band) change which tiles a round visits, never the fixed point: every band,
+    0 (every queued tile each round) included, gives the oracle's fields and best targets."""
+    lib = _lib.load()
+    rng = np.random.default_rng(77)
+    searches = []
+    for k in range(10):
+        rw, rh = int(rng.integers(60, 700)), int(rng.integers(60, 700))
+        searches.append(make_device_search(9700 + k, rw, rh, int(rng.integers(2, 7)), float(rng.integers(8, 33))))
+    old = lib.pcbg_round_band()
+    lib.pcbg_set_round_band(band)
+    try:
+        arr = run_batch(searches)
+        deferred = lib.pcbg_last_batch_deferred()
+    finally:
+        lib.pcbg_set_round_band(old)
+    if band == 0:
+        assert deferred == 0
+    for k, s in enumerate(searches):
+        field, best, bd = oracle_of(s)
+        assert arr[k].best == best, (band, k, arr[k].best, best)
+        if best >= 0:
+            assert arr[k].best_d == bd
+        got = s["out"].cpu().numpy().reshape(s["nl"], s["rh"], s["rw"])
+        assert np.array_equal(got.view(np.uint32), field.view(np.uint32)), (band, k)
+
+
 def test_walkback_matches_oracle(gpu):
     """The device walk-back (one warp per search, after the relaxation) equals the oracle's walk over its exact
     field: the same states in the same order, best target first, ending on the start."""
@@ -366,3 +433,34 @@ def test_concurrent_queries_are_batched_and_exact(gpu):
         assert (out.rx0, out.ry0, out.rw, out.rh, out.best, out.tries) == \
             (ref.rx0, ref.ry0, ref.rw, ref.rh, ref.best, ref.tries)
         assert np.array_equal(out.d.view(np.uint32), ref.d.view(np.uint32))
+
+
+def test_round_cap_stops_the_launch_and_the_device_stays_usable(gpu):
+    """The relaxation's round loop is bounded (pcbg_set_max_rounds lowers the bound): a launch that reaches it stops,
+    the solve returns PCBG_ERR_FAIL with the error bit of the round cap (ERR_ROUNDS = 2), and the next solve on the
+    same context is exact again."""
+    lib = _lib.load()
+    s = make_device_search(9900, 900, 700, 4, 20.0)
+    lib.pcbg_set_max_rounds(2)
+    try:
+        arr = (_lib.Search * 1)()
+        torch = _torch()
+        a = arr[0]
+        a.rw, a.rh, a.nl, a.pitch, a.hpad = s["rw"], s["rh"], s["nl"], s["pitch"], s["hpad"]
+        fac = synth.microbench_factors(s["nl"])
+        for l in range(8):
+            for m in range(8):
+                a.fac[l][m] = float(fac[l, m])
+        a.cf, a.flags, a.vcf = s["cf"].data_ptr(), s["fl"].data_ptr(), s["vcf"].data_ptr()
+        si = s["st"][:1].to(torch.int32)
+        sd = torch.zeros(1, dtype=torch.int64, device="cuda")
+        a.start_idx, a.start_d, a.n_starts = si.data_ptr(), sd.data_ptr(), 1
+        assert lib.pcbg_solve_batch(arr, 1, None) == -1
+        assert "error bits 2" in _lib.last_error(), _lib.last_error()
+    finally:
+        lib.pcbg_set_max_rounds(0)
+    arr = run_batch([s])
+    field, best, bd = oracle_of(s)
+    assert arr[0].best == best
+    got = s["out"].cpu().numpy().reshape(s["nl"], s["rh"], s["rw"])
+    assert np.array_equal(got.view(np.uint32), field.view(np.uint32))
