@@ -272,6 +272,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--no-spec", action="store_true", help="skip the learned-vs-plain speculative batching A/B")
+    ap.add_argument("--no-tune", action="store_true", help="skip the schedule autotuner (untuned rule)")
     ap.add_argument("--band", type=int, default=None,
                     help="relaxation round band (pcbg_set_round_band); default: the library's own")
     ap.add_argument("--cost-maps-only", type=int, nargs=2, metavar=("NX", "NY"), default=None,
@@ -322,6 +323,17 @@ def main():
     dev_waves = [[make(sz) for sz in w] for w in my]
     torch.cuda.synchronize()
 
+    # the library's schedule autotuner (round band and kernel build per layer and batch class), before any timing
+    tune = None
+    if not args.no_tune:
+        ents = (_lib.TuneEntry * 8)()
+        nt = lib.pcbg_autotune(sp, ents, 8)
+        if nt < 0:
+            raise RuntimeError("pcbg_autotune failed: " + _lib.last_error())
+        tune = [{"layers": f"{e.layers_lo}-{e.layers_hi}", "batch_class": e.batch_class, "band": e.band,
+                 "blocks_per_sm": e.blocks_per_sm, "ms": round(e.ms, 3), "ms_untuned": round(e.ms_untuned, 3),
+                 "batch": f"{e.searches} x {e.rw}x{e.rh}x{e.nl}"} for e in ents[:nt]]
+
     def search_array(wave, outs=None):
         arr = (_lib.Search * len(wave))()
         keep = []
@@ -340,6 +352,31 @@ def main():
             a.n_starts = 1
             a.out = outs[k].data_ptr() if outs is not None else None
         return arr, keep
+
+    def batch_fixed_cost(reps=200):
+        """Per-batch fixed cost of pcbg_solve_batch: host time of a call (descriptor staging, copies, clears, the
+        seed / relax / report launches, the result copy and its synchronisation) minus the relaxation's device time,
+        on a batch of one small search (64 x 64 x 2) and on a router-sized batch (two 1024 x 768 x 4 searches)."""
+        res = {}
+        for name, szs in (("one 64x64x2 search", [(64, 64, 2, 12.0, 77)]),
+                          ("two 1024x768x4 searches", [(1024, 768, 4, 12.0, 78), (1024, 768, 4, 20.0, 79)])):
+            w = [make(sz) for sz in szs]
+            arr, _keep = search_array(w)
+            for _ in range(5):
+                lib.pcbg_solve_batch(arr, len(arr), sp)
+            torch.cuda.synchronize()
+            n = reps if len(szs) == 1 else 20
+            wall = relax = 0.0
+            for _ in range(n):
+                t0 = time.perf_counter()
+                if lib.pcbg_solve_batch(arr, len(arr), sp) != 0:
+                    raise RuntimeError(_lib.last_error())
+                wall += time.perf_counter() - t0
+                relax += lib.pcbg_last_batch_kernel_ms() / 1e3
+            res[name] = {"calls": n, "wall_us": round(1e6 * wall / n, 1), "relax_us": round(1e6 * relax / n, 1),
+                         "fixed_us": round(1e6 * (wall - relax) / n, 1),
+                         "fixed_share": round((wall - relax) / wall, 4)}
+        return res
 
     # searches whose source could not be placed are dropped from the wave (none are expected)
     arrays = [search_array(w) for w in dev_waves]
@@ -525,6 +562,8 @@ def main():
                              "state_visits_per_state": round(lv * 1024 / max(1, st_done), 3),
                              "local_iters_per_visit": round(iters[0] / max(1, tv), 3),
                              "round_band": int(lib.pcbg_round_band()),
+                             "blocks_per_sm": int(lib.pcbg_last_batch_blocks_per_sm()),
+                             "autotuned_schedules": tune,
                              "tiles_deferred_per_step": iters[1] // args.steps,
                              "tiles_dropped_per_step": iters[2] // args.steps},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -538,6 +577,7 @@ def main():
                          "kernel": "relax_kernel (persistent tile relaxation)",
                          "kernel_ms_per_step": round(kms / args.steps, 3), "peak_kind": peak_kind},
             "gpu_launches": int(launches),
+            "batch_fixed_cost": None if args.no_spec else batch_fixed_cost(),
             "clocks": clk.summary(),
             "cost_maps": cost_map_roofline(lib, peak),
             "learned_batching": None if args.no_spec else learned_batching(),

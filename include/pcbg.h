@@ -172,7 +172,22 @@ int64_t pcbg_last_batch_settled(void);
  * and drops tiles keyed above the best target found. B = 0 visits every queued tile each round. Results are the
  * same for every B; only the work changes. Default 16. */
 void pcbg_set_round_band(int32_t band);
-int32_t pcbg_round_band(void);
+int32_t pcbg_round_band(void);     /* the band of the last batch solved on this thread */
+/* The schedule autotuner: for each layer-count class (1-2, 3-4, 5-6, 7-8 layers) and batch class (0: fewer than 16
+ * tiles per resident block, as a router's concurrent searches; 1: more, as a round of the batched microbenchmark)
+ * it solves seeded searches on `stream` under every round band (0, 4, 8, 16, 32) and kernel build (2 or 3 blocks
+ * per SM), and keeps the fastest for every later launch of that class (pcbg_set_round_band still overrides the band).
+ * Writes one entry per class (up to cap) and returns how many, or PCBG_ERR_FAIL. Takes a few seconds. */
+typedef struct pcbg_tune_entry {
+    int32_t layers_lo, layers_hi, batch_class;
+    int32_t band, blocks_per_sm;      /* the schedule chosen */
+    float ms, ms_untuned;             /* its relaxation time, and the untuned rule's (band 16, 2 / 3 blocks) */
+    int32_t searches, rw, rh, nl;     /* the timed batch */
+} pcbg_tune_entry;
+int32_t pcbg_autotune(void* stream, pcbg_tune_entry* out, int32_t cap);
+/* Resident blocks per SM of the last batch's relaxation launch on this thread. */
+int32_t pcbg_last_batch_blocks_per_sm(void);
+
 /* Cap on the relaxation rounds of one launch (default 2^20; a value < 1 restores it). A launch that reaches the cap
  * stops and its solve returns PCBG_ERR_FAIL: a bounded device loop, which tests lower to see the error path. */
 void pcbg_set_max_rounds(int32_t rounds);

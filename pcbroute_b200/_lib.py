@@ -26,7 +26,8 @@ PCBG_SYMBOLS = [
     "pcbg_set_max_rounds", "pcbg_last_batch_settled", "pcbg_mirror_class", "pcbg_mirror_spans",
     "pcbg_mirror_history", "pcbg_mirror_download", "pcbg_sched_add_log_host", "pcbg_rsched_mode",
     "pcbg_rsched_begin", "pcbg_rsched_net", "pcbg_rsched_allow", "pcbg_rsched_started", "pcbg_rsched_committed",
-    "pcbg_rsched_verdict", "pcbg_rsched_end", "pcbg_rsched_get_stats",
+    "pcbg_rsched_verdict", "pcbg_rsched_end", "pcbg_rsched_get_stats", "pcbg_autotune",
+    "pcbg_last_batch_blocks_per_sm",
     "pcbg_synth_search_host", "pcbg_costs_create", "pcbg_costs_destroy", "pcbg_costs_set_static",
     "pcbg_costs_set_occupancy", "pcbg_costs_set_history", "pcbg_costs_set_ground", "pcbg_costs_rebuild",
     "pcbg_costs_stamp", "pcbg_costs_add_history", "pcbg_costs_download", "pcbg_costs_download_history",
@@ -40,6 +41,12 @@ GPU_H_SYMBOLS = [
     "_ZN6GpuOut7reserveEm",                      # void GpuOut::reserve(size_t)
     "_ZNK6GpuOutclEl",                           # float GpuOut::operator()(int64_t) const
 ]
+
+
+class TuneEntry(C.Structure):
+    _fields_ = [("layers_lo", C.c_int32), ("layers_hi", C.c_int32), ("batch_class", C.c_int32), ("band", C.c_int32),
+                ("blocks_per_sm", C.c_int32), ("ms", C.c_float), ("ms_untuned", C.c_float), ("searches", C.c_int32),
+                ("rw", C.c_int32), ("rh", C.c_int32), ("nl", C.c_int32)]
 
 
 class Query(C.Structure):
@@ -152,6 +159,9 @@ def load() -> C.CDLL:
     lib.pcbg_mirror_download.restype = C.c_int
     lib.pcbg_sched_add_log_host.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64]
     lib.pcbg_sched_add_log_host.restype = C.c_int
+    lib.pcbg_autotune.argtypes = [C.c_void_p, C.c_void_p, C.c_int32]
+    lib.pcbg_autotune.restype = C.c_int32
+    lib.pcbg_last_batch_blocks_per_sm.restype = C.c_int32
     lib.pcbg_set_round_band.argtypes = [C.c_int32]
     lib.pcbg_set_round_band.restype = None
     lib.pcbg_round_band.restype = C.c_int32

@@ -921,7 +921,7 @@ __global__ void __launch_bounds__(NT, MINB) relax_kernel(SolveArgs a) {
             const int vp = round & 1;
             if (blockIdx.x == 0 && tid == 0) { a.ctl[C_VCNT + (vp ^ 1)] = 0; a.ctl[C_VNEXT + (vp ^ 1)] = 0; }
             for (int q = blockIdx.x * NT + tid; q < a.n; q += nblocks * NT) a.st[q].kmin[(round + 2) % 3] = KEY_NONE;
-            unsigned long long deferred = 0, dropped = 0;
+            unsigned int deferred = 0, dropped = 0;
             for (unsigned int k = blockIdx.x * NT + tid; k < cnt; k += nblocks * NT) {
                 const unsigned long long it = __ldcg(items + k);
                 const int s = int(it >> 32), tile = int(it & 0xFFFFFFFFu);
@@ -943,8 +943,10 @@ __global__ void __launch_bounds__(NT, MINB) relax_kernel(SolveArgs a) {
                 const unsigned int pos = atomicAdd(a.ctl + C_VCNT + vp, 1u);
                 a.vl[pos] = it;
             }
-            if (deferred) atomicAdd(a.visits + 3, deferred);
-            if (dropped) atomicAdd(a.visits + 4, dropped);
+            deferred = __reduce_add_sync(0xFFFFFFFFu, deferred);
+            dropped = __reduce_add_sync(0xFFFFFFFFu, dropped);
+            if ((tid & 31) == 0 && deferred) atomicAdd(a.visits + 3, static_cast<unsigned long long>(deferred));
+            if ((tid & 31) == 0 && dropped) atomicAdd(a.visits + 4, static_cast<unsigned long long>(dropped));
             grid_barrier(a.ctl, nblocks);
             items = a.vl;
             next = a.ctl + C_VNEXT + vp;
@@ -1135,9 +1137,6 @@ struct Arena {
     DevBuf dist, stamp, tkey, wl, vl, sdev, sstat, ctl, visits, sptr;
 } g_arena;
 
-// Band of an ordered round, in multiples of a search's weight scale (the cost of one step through open board);
-// 0 runs every queued tile each round. Set by pcbg_set_round_band or the autotuner.
-int g_band = 16;
 // Round cap of a launch: a bound on the device loop, which tests lower (pcbg_set_max_rounds, or PCBG_MAX_ROUNDS in
 // the environment of a process such as the router) to see a launch stop with ERR_ROUNDS and its caller fall back.
 int max_rounds_from_env() {
@@ -1184,16 +1183,52 @@ struct RelaxLaunch {
     void* fn;
     int resident;
 };
-template <typename DT> RelaxLaunch relax_launch(size_t smem, size_t tiles) {
+int sm_count() {
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (tiles >= size_t(16) * 3 * sms) {
+    return sms > 0 ? sms : 1;
+}
+
+// minb: the build asked for (3 or 2 blocks per SM; 0: the untuned rule, 3 for batches of at least 16 tiles per
+// resident block). A 3-block build whose shared memory does not fit 3 blocks falls back to the 2-block one.
+template <typename DT> RelaxLaunch relax_launch(size_t smem, size_t tiles, int minb = 0) {
+    const int sms = sm_count();
+    if (minb == 3 || (minb == 0 && tiles >= size_t(16) * 3 * sms)) {
         const int p3 = blocks_per_sm<DT, 3>(smem);
         if (p3 >= 3) return {reinterpret_cast<void*>(relax_kernel<DT, 3>), p3 * sms};
     }
     const int p2 = blocks_per_sm<DT, 2>(smem);
     return {reinterpret_cast<void*>(relax_kernel<DT, 2>), p2 < 0 ? -1 : p2 * sms};
+}
+
+// ---- relaxation schedules: the round band and the kernel build of a launch, per layer-count class (1-2, 3-4, 5-6,
+// 7-8 layers) and batch class (fewer, or at least, 16 tiles per resident block of the 3-block build)
+
+struct Schedule {
+    int band;
+    int minb;
+};
+struct TuneTable {
+    bool valid = false;
+    Schedule s[4][2];
+    float ms[4][2];
+    float ms_untuned[4][2];
+};
+TuneTable g_tune;
+int g_band_user = -1;                 // pcbg_set_round_band: one band for every launch (-1: tuned or default)
+constexpr int DEFAULT_BAND = 16;
+const Schedule* g_force = nullptr;    // the autotuner's candidate while it times one
+
+int layer_class(int nl) { return std::min(3, std::max(0, (nl - 1) / 2)); }
+int size_class(size_t tiles) { return tiles >= size_t(16) * 3 * sm_count() ? 1 : 0; }
+
+Schedule schedule_for(int nl, size_t tiles) {
+    if (g_force) return *g_force;
+    Schedule sc{DEFAULT_BAND, 0};
+    if (g_tune.valid) sc = g_tune.s[layer_class(nl)][size_class(tiles)];
+    if (g_band_user >= 0) sc.band = g_band_user;
+    return sc;
 }
 
 // joint mode needs one factor per move class on every layer (true of every query the router builds)
@@ -1305,11 +1340,16 @@ int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream
     a.cap = cap;
     a.ctl = static_cast<unsigned int*>(A.ctl.p);
     a.visits = static_cast<unsigned long long*>(A.visits.p);
+    const Schedule sc = schedule_for(nlmax, tiles);
+    if (sizeof(DT) != 4) band = 0;
+    else if (band < 0) band = sc.band;
     a.max_rounds = g_max_rounds;
     a.band = unsigned(band);
-    a.ordered = sizeof(DT) == 4 && band > 0 ? 1 : 0;
+    a.ordered = band > 0 ? 1 : 0;
     seed_kernel<DT><<<m, 128, 0, stream>>>(a, d_sip, d_sdp, d_ns);
-    const RelaxLaunch R = relax_launch<DT>(smem, tiles);
+    const RelaxLaunch R = relax_launch<DT>(smem, tiles, sc.minb);
+    bs.band = band;
+    bs.blocks_per_sm = R.resident / sm_count();
     if (R.resident <= 0) { t_err = "relax kernel cannot be resident"; return -1; }
     // a round visits each queued tile once: more blocks than tiles would only wait at the grid barriers
     const int blocks = int(std::min<size_t>(size_t(R.resident), std::max<size_t>(tiles, 1)));
@@ -1373,8 +1413,14 @@ void set_error(const std::string& s) { t_err = s; }
 const std::string& last_error() { return t_err; }
 BatchStats& last_stats() { return t_stats; }
 
+int solve_batch_locked(BatchItem* items, int n, cudaStream_t stream);
+
 int solve_batch(BatchItem* items, int n, cudaStream_t stream) {
     std::lock_guard<std::mutex> g(g_mu);
+    return solve_batch_locked(items, n, stream);
+}
+
+int solve_batch_locked(BatchItem* items, int n, cudaStream_t stream) {
     t_stats = BatchStats{};
     if (n <= 0) return 0;
     for (int k = 0; k < n; ++k) {
@@ -1387,7 +1433,7 @@ int solve_batch(BatchItem* items, int n, cudaStream_t stream) {
     }
     std::vector<int> all(n);
     for (int k = 0; k < n; ++k) all[k] = k;
-    if (run_batch<uint32_t>(items, all, stream, t_stats, g_band) != 0) return -1;
+    if (run_batch<uint32_t>(items, all, stream, t_stats, -1) != 0) return -1;
     std::vector<int> wide;
     for (int k = 0; k < n; ++k)
         if (items[k].status == 1) wide.push_back(k);
@@ -1437,9 +1483,10 @@ extern "C" int64_t pcbg_last_batch_settled(void) { return pcbg::last_stats().set
 
 extern "C" void pcbg_set_round_band(int32_t band) {
     std::lock_guard<std::mutex> g(pcbg::g_mu);
-    pcbg::g_band = band < 0 ? 0 : band;
+    pcbg::g_band_user = band < 0 ? -1 : band;
 }
-extern "C" int32_t pcbg_round_band(void) { return pcbg::g_band; }
+extern "C" int32_t pcbg_round_band(void) { return pcbg::last_stats().band; }
+extern "C" int32_t pcbg_last_batch_blocks_per_sm(void) { return pcbg::last_stats().blocks_per_sm; }
 
 extern "C" void pcbg_set_max_rounds(int32_t rounds) {
     std::lock_guard<std::mutex> g(pcbg::g_mu);
@@ -1500,7 +1547,7 @@ unsigned char* na_base() {
 }
 
 template <typename DT>
-int na_run(pcbg_search* q, unsigned char* base, cudaStream_t stream, int band) {
+int na_run(pcbg_search* q, unsigned char* base, cudaStream_t stream, int band, int minb) {
     SDev S;
     memset(&S, 0, sizeof(S));
     S.rw = q->rw; S.rh = q->rh; S.nl = q->nl; S.pitch = q->pitch; S.hpad = q->hpad;
@@ -1517,7 +1564,7 @@ int na_run(pcbg_search* q, unsigned char* base, cudaStream_t stream, int band) {
     const size_t states = size_t(q->nl) * q->hpad * q->pitch, tiles = size_t(S.ntx) * S.nty;
     // the launch shape first: nothing is queued on the stream unless the relaxation can be launched
     const size_t smem = S.mode ? layout(q->nl, joint_wbytes(S.K), 4).total : layout(q->nl, 4, sizeof(DT)).total;
-    const RelaxLaunch R = relax_launch<DT>(smem, tiles);
+    const RelaxLaunch R = relax_launch<DT>(smem, tiles, minb);
     if (R.resident <= 0) { na_error("relax kernel cannot be resident%s"); return -1; }
     // a round visits each queued tile once: more blocks than tiles would only wait at the grid barriers
     const int blocks = int(std::min<size_t>(size_t(R.resident), std::max<size_t>(tiles, 1)));
@@ -1611,10 +1658,100 @@ extern "C" int pcbg_solve_noalloc(pcbg_search* s, void* stream) {
     if (!base) return PCBG_ERR_FAIL;
     std::lock_guard<std::mutex> g(g_mu);  // one solve at a time in this process: calls share the array
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    if (na_run<uint32_t>(s, base, st, g_band) != 0) return PCBG_ERR_FAIL;
+    const Schedule sc = schedule_for(s->nl, size_t(s->pitch / TILE) * (s->hpad / TILE));
+    if (na_run<uint32_t>(s, base, st, sc.band, sc.minb) != 0) return PCBG_ERR_FAIL;
     if (s->status == 1) {
-        if (na_run<uint64_t>(s, base, st, 0) != 0) return PCBG_ERR_FAIL;
+        if (na_run<uint64_t>(s, base, st, 0, sc.minb) != 0) return PCBG_ERR_FAIL;
         s->status = 1;
     }
     return 0;
+}
+
+// ---- the schedule autotuner ----
+//
+// For each layer-count class (searches of 2, 4, 6, 8 layers) and batch class (two searches of 1024 x 768, the size
+// of a router's few concurrent searches; and enough 512 x 512 searches for at least 16 tiles per resident block, a
+// round of the batched microbenchmark), the seeded generator's searches are solved under every schedule: round
+// band 0 (every queued tile each round), 4, 8, 16, 32 weight scales, and the 2- and 3-blocks-per-SM builds. The
+// fastest relaxation (least device time of two launches) becomes the class's schedule for every later launch.
+// Results never depend on the schedule; only the time does.
+
+extern "C" int32_t pcbg_autotune(void* stream, pcbg_tune_entry* out, int32_t cap) {
+    using namespace pcbg;
+    std::lock_guard<std::mutex> g(g_mu);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int sms = sm_count();
+    const int bands[] = {0, 4, 8, 16, 32};
+    const int nls[4] = {2, 4, 6, 8};
+    TuneTable T;
+    int written = 0;
+    for (int lc = 0; lc < 4; ++lc)
+        for (int sc = 0; sc < 2; ++sc) {
+            const int nl = nls[lc];
+            const int rw = sc ? 512 : 1024, rh = sc ? 512 : 768;
+            const int n = sc ? int((size_t(16) * 3 * sms + 255) / 256 * 11 / 10) : 2;
+            const size_t plane = size_t(rw) * rh, PN = plane * nl;
+            // one allocation: per search cf, flags, vcf, the generator's source / target, the start cost
+            const size_t per = PN * 4 + PN + plane * 4 + 16 + 16;
+            unsigned char* buf = nullptr;
+            if (cudaMalloc(&buf, per * n) != cudaSuccess) { set_error("autotune allocation failed"); return PCBG_ERR_FAIL; }
+            std::vector<BatchItem> items(n);
+            bool ok = true;
+            for (int k = 0; k < n && ok; ++k) {
+                unsigned char* b = buf + per * k;
+                float* cf = reinterpret_cast<float*>(b);
+                uint8_t* fl = b + PN * 4;
+                float* vcf = reinterpret_cast<float*>(b + PN * 5);
+                int64_t* stt = reinterpret_cast<int64_t*>(b + PN * 5 + plane * 4);
+                uint64_t* sd = reinterpret_cast<uint64_t*>(stt + 2);
+                ok = pcbg_synth_search(0xA0707E00ull + 97 * k + lc * 7 + sc, rw, rh, nl, rw, rh, 8.0f + float(k % 25),
+                                       cf, fl, vcf, stt, st) == 0;
+                cudaMemsetAsync(sd, 0, 8, st);
+                BatchItem& it = items[k];
+                memset(&it, 0, sizeof(it));
+                it.rw = rw; it.rh = rh; it.nl = nl; it.pitch = rw; it.hpad = rh;
+                for (int l = 0; l < MAX_LAYERS; ++l)
+                    for (int m = 0; m < 8; ++m) it.fac[l][m] = m < 4 ? 1.0f : 1.41421354f;
+                it.cf = cf; it.fl = fl; it.vcf = vcf;
+                // the start: the generator's source, a rect state in the low word of its int64 (little endian); a
+                // source that could not be placed (-1) is beyond the search and seeds nothing
+                it.start_idx = reinterpret_cast<const uint32_t*>(stt);
+                it.start_d = sd;
+                it.n_starts = 1;
+            }
+            if (!ok || cudaStreamSynchronize(st) != cudaSuccess) {
+                cudaFree(buf);
+                set_error("autotune search generation failed");
+                return PCBG_ERR_FAIL;
+            }
+            float best_ms = 1e30f, untuned_ms = 1e30f;
+            Schedule best{DEFAULT_BAND, 0};
+            for (int band : bands)
+                for (int minb = 2; minb <= 3; ++minb) {
+                    const Schedule cand{band, minb};
+                    g_force = &cand;
+                    float ms = 1e30f;
+                    for (int rep = 0; rep < 2; ++rep) {
+                        if (solve_batch_locked(items.data(), n, st) != 0) { ms = 1e30f; break; }
+                        ms = std::min(ms, t_stats.kernel_ms);
+                    }
+                    g_force = nullptr;
+                    if (ms < best_ms) { best_ms = ms; best = cand; }
+                    if (band == DEFAULT_BAND && minb == (sc ? 3 : 2)) untuned_ms = ms;
+                }
+            cudaFree(buf);
+            T.s[lc][sc] = best;
+            T.ms[lc][sc] = best_ms;
+            T.ms_untuned[lc][sc] = untuned_ms;
+            if (out && written < cap) {
+                pcbg_tune_entry& e = out[written++];
+                e.layers_lo = 2 * lc + 1; e.layers_hi = 2 * lc + 2; e.batch_class = sc;
+                e.band = best.band; e.blocks_per_sm = best.minb;
+                e.ms = best_ms; e.ms_untuned = untuned_ms;
+                e.searches = n; e.rw = rw; e.rh = rh; e.nl = nl;
+            }
+        }
+    T.valid = true;
+    g_tune = T;
+    return written;
 }
