@@ -92,9 +92,10 @@ def test_oracle_backend_engaged_walks_back_every_search(cfg, seed):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("cfg,seed", BOARDS)
+@pytest.mark.parametrize("cfg,seed", BOARDS + [("c1", 1)])
 def test_b200_router_sessions_match_the_oracle_router(cfg, seed):
-    """(ii): the same session bytes and --eval line with the oracle and the B200 back end, engaged on every search."""
+    """(ii): the same session bytes and --eval line with the oracle and the B200 back end, engaged on every search,
+    at -mt 1 and with 16 workers (the seeded 50 x 40 mm, 2-layer c1 board included)."""
     board = dsngen.generate(cfg, seed)
     o = route(_bin("pcbroute_oracle"), board, "-mt", "1", "-v", "--gpu-pops", "1")
     g = route(_bin("pcbroute_b200"), board, "-mt", "1", "-v", "--gpu-pops", "1")
@@ -102,8 +103,8 @@ def test_b200_router_sessions_match_the_oracle_router(cfg, seed):
     assert _gpu_count(g[0]) == _gpu_count(o[0])
     assert o[1] and g[1] == o[1]
     assert g[2] == o[2]
-    g4 = route(_bin("pcbroute_b200"), board, "-mt", "4", "-v", "--gpu-pops", "1")
-    assert g4[1] == o[1] and g4[2] == o[2]
+    g16 = route(_bin("pcbroute_b200"), board, "-mt", "16", "--gpu-slots", "16", "-v", "--gpu-pops", "1")
+    assert g16[1] == o[1] and g16[2] == o[2]
 
 
 def _failed(err):
