@@ -175,7 +175,7 @@ void pcbg_set_round_band(int32_t band);
 int32_t pcbg_round_band(void);     /* the band of the last batch solved on this thread */
 /* The schedule autotuner: for each layer-count class (1-2, 3-4, 5-6, 7-8 layers) and batch class (0: fewer than 16
  * tiles per resident block, as a router's concurrent searches; 1: more, as a round of the batched microbenchmark)
- * it solves seeded searches on `stream` under every round band (0, 4, 8, 16, 32) and kernel build (2 or 3 blocks
+ * it solves seeded searches on `stream` under every round band (0, 8, 16, 32, 64, 128) and kernel build (2 or 3 blocks
  * per SM), and keeps the fastest for every later launch of that class (pcbg_set_round_band still overrides the band).
  * Writes one entry per class (up to cap) and returns how many, or PCBG_ERR_FAIL. Takes a few seconds. */
 typedef struct pcbg_tune_entry {

@@ -1672,7 +1672,7 @@ extern "C" int pcbg_solve_noalloc(pcbg_search* s, void* stream) {
 // For each layer-count class (searches of 2, 4, 6, 8 layers) and batch class (two searches of 1024 x 768, the size
 // of a router's few concurrent searches; and enough 512 x 512 searches for at least 16 tiles per resident block, a
 // round of the batched microbenchmark), the seeded generator's searches are solved under every schedule: round
-// band 0 (every queued tile each round), 4, 8, 16, 32 weight scales, and the 2- and 3-blocks-per-SM builds. The
+// band 0 (every queued tile each round), 8, 16, 32, 64, 128 weight scales, and the 2- and 3-blocks-per-SM builds. The
 // fastest relaxation (least device time of two launches) becomes the class's schedule for every later launch.
 // Results never depend on the schedule; only the time does.
 
@@ -1681,7 +1681,7 @@ extern "C" int32_t pcbg_autotune(void* stream, pcbg_tune_entry* out, int32_t cap
     std::lock_guard<std::mutex> g(g_mu);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int sms = sm_count();
-    const int bands[] = {0, 4, 8, 16, 32};
+    const int bands[] = {0, 8, 16, 32, 64, 128};
     const int nls[4] = {2, 4, 6, 8};
     TuneTable T;
     int written = 0;
