@@ -1217,15 +1217,17 @@ struct TuneTable {
 };
 TuneTable g_tune;
 int g_band_user = -1;                 // pcbg_set_round_band: one band for every launch (-1: tuned or default)
-constexpr int DEFAULT_BAND = 16;
+constexpr int DEFAULT_BAND = 16;    // the band the untuned rule of the first ordered kernel used (reported as "untuned")
 const Schedule* g_force = nullptr;    // the autotuner's candidate while it times one
 
 int layer_class(int nl) { return std::min(3, std::max(0, (nl - 1) / 2)); }
 int size_class(size_t tiles) { return tiles >= size_t(16) * 3 * sm_count() ? 1 : 0; }
 
+// Before (or without) a tuning run: what the tuner chose on a B200 for most classes (profiles/
+// relax_kernel_round_schedules.md): small batches unordered on the 2-block build, large ones with a band of 32.
 Schedule schedule_for(int nl, size_t tiles) {
     if (g_force) return *g_force;
-    Schedule sc{DEFAULT_BAND, 0};
+    Schedule sc = size_class(tiles) ? Schedule{32, 0} : Schedule{0, 2};
     if (g_tune.valid) sc = g_tune.s[layer_class(nl)][size_class(tiles)];
     if (g_band_user >= 0) sc.band = g_band_user;
     return sc;
