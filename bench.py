@@ -42,9 +42,9 @@ WORKLOAD = ("batched-search microbenchmark: 4096 seeded single-source single-tar
 # where a tile visit stages 32 x 32 states of each of its search's layers. The per-solved-state figure counts the
 # same 12 bytes once per state of the windows solved.
 BYTES_PER_STATE_VISIT = 12
-# DRAM bytes moved per algorithmic byte by relax_kernel, from one ncu capture of the 64-search case (profiles/
-# relax_kernel_microbench.md). A full wave is too large to capture; its traffic grows with the state visits, so the
-# bench scales this ratio by the launch's algorithmic bytes.
+# DRAM bytes moved per algorithmic byte by relax_kernel, from one ncu capture of the 64-search case
+# (dram__bytes_read.sum + dram__bytes_write.sum over 12 B per state visit). A full wave is too large to capture; its
+# traffic grows with the state visits, so the bench scales this ratio by the launch's algorithmic bytes.
 NCU_TRAFFIC_PER_ALG_BYTE = 1.11
 
 

@@ -1223,8 +1223,8 @@ const Schedule* g_force = nullptr;    // the autotuner's candidate while it time
 int layer_class(int nl) { return std::min(3, std::max(0, (nl - 1) / 2)); }
 int size_class(size_t tiles) { return tiles >= size_t(16) * 3 * sm_count() ? 1 : 0; }
 
-// Before (or without) a tuning run: what the tuner chose on a B200 for most classes (profiles/
-// relax_kernel_round_schedules.md): small batches unordered on the 2-block build, large ones with a band of 32.
+// Before (or without) a tuning run: what the tuner chose on a B200 for most classes: small batches unordered on the
+// 2-block build, large ones with a band of 32.
 Schedule schedule_for(int nl, size_t tiles) {
     if (g_force) return *g_force;
     Schedule sc = size_class(tiles) ? Schedule{32, 0} : Schedule{0, 2};
