@@ -80,15 +80,15 @@ def board_file(d, spec):
     return path
 
 
-def train(d, specs, mt, timeout):
+def train(d, specs, mt, timeout, extra, emit):
     """Conflict logs of b200x runs in log mode over the training boards, then the predictor fitted on the GPU."""
     from pcbroute_b200 import sched
     logs = []
     for spec in specs:
         log = os.path.join(d, f"log_{spec.replace(':', '_')}.bin")
-        res = run("pcbroute_b200x", board_file(d, spec), ["-mt", str(mt), "--gpu-pops", "1"], timeout,
-                  {"PCBG_SCHED": "log", "PCBG_SCHED_LOG": log})
-        print(json.dumps({"train_board": spec, "arm": "b200x log", **res}), flush=True)
+        args = ["-mt", str(mt), "--gpu-slots", str(mt), "--gpu-pops", "1", *extra]
+        res = run("pcbroute_b200x", board_file(d, spec), args, timeout, {"PCBG_SCHED": "log", "PCBG_SCHED_LOG": log})
+        emit({"train_board": spec, "arm": "b200x log", "args": " ".join(args), **res})
         if os.path.exists(log):
             logs.append(log)
     model = os.path.join(d, "model.bin")
@@ -107,10 +107,12 @@ def main():
     ap.add_argument("--cpu1", action="store_true", help="also run the CPU router at -mt 1")
     ap.add_argument("--timeout", type=int, default=1800)
     ap.add_argument("--out", default=None, help="also write the JSON lines here")
+    ap.add_argument("--router-args", default="", help="options given to every run, e.g. \"-it 2 --ripups 0\"")
     a = ap.parse_args()
     cores = os.cpu_count() or 1
     mt = a.mt or cores
     arms = a.arms.split(",")
+    extra = a.router_args.split()
     out = open(a.out, "a") if a.out else None
 
     def emit(line):
@@ -122,7 +124,7 @@ def main():
     with tempfile.TemporaryDirectory() as d:
         model = a.model
         if "learned" in arms and not model:
-            model, info = train(d, [s for s in a.train.split(",") if s], mt, a.timeout)
+            model, info = train(d, [s for s in a.train.split(",") if s], mt, a.timeout, extra, emit)
             emit({"trained": info, "boards": a.train})
         plan = []
         if "cpu" in arms:
@@ -141,6 +143,7 @@ def main():
         for spec in a.boards.split(","):
             dsn = board_file(d, spec)
             for arm, binary, args, env in plan:
+                args = args + extra
                 res = run(binary, dsn, args, a.timeout, env)
                 emit({"board": spec, "arm": arm, "args": " ".join(args), "cores": cores, **res})
 
