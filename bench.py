@@ -379,7 +379,20 @@ def main():
         return res
 
     # searches whose source could not be placed are dropped from the wave (none are expected)
-    arrays = [search_array(w) for w in dev_waves]
+    # every step writes its reported fields: one device buffer, the size of the largest wave, that each wave's
+    # searches fill (a caller that keeps its fields on the device reuses its buffer the same way)
+    field_n = max(sum(sr["rw"] * sr["rh"] * sr["nl"] for sr in w) for w in dev_waves)
+    field_buf = torch.empty(field_n, dtype=torch.float32, device="cuda")
+
+    def field_views(w):
+        views, o = [], 0
+        for sr in w:
+            m = sr["rw"] * sr["rh"] * sr["nl"]
+            views.append(field_buf[o:o + m])
+            o += m
+        return views
+
+    arrays = [search_array(w, field_views(w)) for w in dev_waves]
     states = [sum(s["rw"] * s["rh"] * s["nl"] for s in w) for w in dev_waves]
 
     iters = [0, 0, 0, 0]
@@ -554,6 +567,8 @@ def main():
             "config": config_of(args),
             "parallelism": f"replicas x{ws}",
             "l2": "inputs larger than L2 (several GB per wave)",
+            "timed_step": "one pcbg_solve_batch of a resident wave: clears, seeds, the relaxation launch, the report "
+                          "kernel writing every search's field to device memory, the results back to the host",
             "reported_states": {"value": round(9.0 * settled_all / (ms_max / 1e3) / 1e9, 4), "unit": UNIT,
                                 "states_per_step": int(settled_all // args.steps),
                                 "definition": "9 x the states at or below each search's best target cost, per second"},
