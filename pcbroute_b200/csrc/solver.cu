@@ -55,7 +55,10 @@ constexpr uint32_t KEY_NONE = 0xFFFFFFFFu;   // tile key / round minimum: nothin
 
 // control words of a batch: per rotating round the queued count and the next item taken; per round parity the
 // count and next item of the round's visit list (ordered rounds)
-enum { C_CNT = 0, C_NEXT = 3, C_BAR = 6, C_GEN = 7, C_ERR = 8, C_ROUNDS = 9, C_VCNT = 10, C_VNEXT = 12, C_N = 16 };
+// (C_WIDEN: the doublings of the band the next ordered round uses)
+enum { C_CNT = 0, C_NEXT = 3, C_BAR = 6, C_GEN = 7, C_ERR = 8, C_ROUNDS = 9, C_VCNT = 10, C_VNEXT = 12, C_WIDEN = 14,
+       C_N = 16 };
+constexpr unsigned int MAX_WIDEN = 12;   // band x 4096: wider than any search's key range, i.e. unordered
 enum { ERR_BARRIER = 1, ERR_ROUNDS = 2, ERR_OVERFLOW = 4 };
 // counters of a launch: tile visits, layer visits, local iterations, tiles deferred to a later round, tiles dropped
 constexpr int NVIS = 5;
@@ -919,6 +922,8 @@ __global__ void __launch_bounds__(NT, MINB) relax_kernel(SolveArgs a) {
             // can matter; one keyed above the search's band waits for a later round (listed again, its key and
             // the next round's least key kept). The rest make the visit list.
             const int vp = round & 1;
+            const unsigned int widen = *reinterpret_cast<volatile unsigned int*>(a.ctl + C_WIDEN);
+            const unsigned long long band = static_cast<unsigned long long>(a.band) << widen;
             if (blockIdx.x == 0 && tid == 0) { a.ctl[C_VCNT + (vp ^ 1)] = 0; a.ctl[C_VNEXT + (vp ^ 1)] = 0; }
             for (int q = blockIdx.x * NT + tid; q < a.n; q += nblocks * NT) a.st[q].kmin[(round + 2) % 3] = KEY_NONE;
             unsigned int deferred = 0, dropped = 0;
@@ -934,7 +939,7 @@ __global__ void __launch_bounds__(NT, MINB) relax_kernel(SolveArgs a) {
                 const uint32_t km = *reinterpret_cast<const volatile unsigned int*>(&st.kmin[buf]);
                 const uint32_t ws = *reinterpret_cast<const volatile unsigned int*>(&st.wscale);
                 const unsigned long long thr = ws == KEY_NONE || km == KEY_NONE
-                    ? ~0ull : static_cast<unsigned long long>(km) + static_cast<unsigned long long>(ws) * a.band;
+                    ? ~0ull : static_cast<unsigned long long>(km) + static_cast<unsigned long long>(ws) * band;
                 if (key > thr) {
                     queue_tile(a, S, s, tile, round + 1, key);
                     ++deferred;
@@ -951,6 +956,15 @@ __global__ void __launch_bounds__(NT, MINB) relax_kernel(SolveArgs a) {
             items = a.vl;
             next = a.ctl + C_VNEXT + vp;
             vcnt = *reinterpret_cast<volatile unsigned int*>(a.ctl + C_VCNT + vp);
+            // A round whose visit list cannot keep every block busy widens the next round's band (doubling it, up
+            // to unordered); a round with far more tiles than blocks narrows it again. Read by every block only
+            // after the end-of-round barrier, so the whole grid uses one band per round.
+            if (blockIdx.x == 0 && tid == 0) {
+                unsigned int w = widen;
+                if (vcnt < 2 * nblocks) w = w < MAX_WIDEN ? w + 1 : w;
+                else if (vcnt > 16 * nblocks && w > 0) w -= 1;
+                a.ctl[C_WIDEN] = w;
+            }
         }
         for (;;) {
             if (tid == 0) {
