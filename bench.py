@@ -171,6 +171,33 @@ def learned_batching():
     return out
 
 
+def route_seconds():
+    """The router-level figures of the metric's first half (route s, plain GPU against learned-batched GPU), as
+    baseline/route_times.py measured them on a B200 and committed them beside the ncu summaries: routing a seeded
+    board takes minutes per arm, longer than this benchmark's run, so they are read, not re-measured, and the
+    source says where they come from."""
+    out = {}
+    for board in ("c1", "c2"):
+        path = os.path.join(ROOT, "profiles", f"router_route_times_{board}.txt")
+        if not os.path.exists(path):
+            continue
+        arms = {}
+        for ln in open(path):
+            d = json.loads(ln)
+            if "arm" not in d or "board" not in d:
+                continue
+            arms[d["arm"]] = {"route_s": d["route_s"], "wasted_fraction": d["wasted_fraction"],
+                              "gpu_searches": d["gpu_searches"], "ses_sha256": d["ses_sha256"], "args": d["args"],
+                              "cores": d["cores"]}
+        if arms:
+            out[board] = arms
+    if not out:
+        return None
+    out["source"] = ("profiles/router_route_times.md: python baseline/route_times.py --arms cpu,refgpu,b200,b200x,"
+                     "learned on one B200 box (16 host cores)")
+    return out
+
+
 def dist_setup():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -599,6 +626,7 @@ def main():
             "plain_gpu": None if args.no_spec else plain_gpu_comparison(),
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "route_s": route_seconds(),
         }
         print(json.dumps(line), flush=True)
     if ws > 1:
