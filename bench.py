@@ -420,6 +420,15 @@ def main():
         return views
 
     arrays = [search_array(w, field_views(w)) for w in dev_waves]
+    # and on this run's own first wave (solved 24 times, untimed): its class's schedule for the timed steps
+    if not args.no_tune:
+        e = _lib.TuneEntry()
+        arr0, _ = arrays[0]
+        if lib.pcbg_autotune_batch(arr0, len(arr0), sp, C.byref(e)) != 1:
+            raise RuntimeError("pcbg_autotune_batch failed: " + _lib.last_error())
+        tune.append({"layers": f"{e.layers_lo}-{e.layers_hi}", "batch_class": e.batch_class, "band": e.band,
+                     "blocks_per_sm": e.blocks_per_sm, "ms": round(e.ms, 3), "ms_untuned": round(e.ms_untuned, 3),
+                     "batch": f"wave 0 of this run ({e.searches} searches, up to {e.nl} layers)"})
     states = [sum(s["rw"] * s["rh"] * s["nl"] for s in w) for w in dev_waves]
 
     iters = [0, 0, 0, 0]

@@ -185,6 +185,10 @@ typedef struct pcbg_tune_entry {
     int32_t searches, rw, rh, nl;     /* the timed batch */
 } pcbg_tune_entry;
 int32_t pcbg_autotune(void* stream, pcbg_tune_entry* out, int32_t cap);
+/* The same on the caller's own batch (as pcbg_solve_batch takes it; it is solved 24 times): the fastest schedule
+ * becomes the one of the batch's class, for callers whose batches repeat in shape. Returns 1 (entry in *out, rw / rh
+ * 0 for a mixed batch) or PCBG_ERR_FAIL. */
+int32_t pcbg_autotune_batch(pcbg_search* s, int32_t n, void* stream, pcbg_tune_entry* out);
 /* Resident blocks per SM of the last batch's relaxation launch on this thread. */
 int32_t pcbg_last_batch_blocks_per_sm(void);
 

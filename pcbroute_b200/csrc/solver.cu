@@ -1224,7 +1224,7 @@ struct Schedule {
     int minb;
 };
 struct TuneTable {
-    bool valid = false;
+    bool set[4][2] = {};
     Schedule s[4][2];
     float ms[4][2];
     float ms_untuned[4][2];
@@ -1242,7 +1242,7 @@ int size_class(size_t tiles) { return tiles >= size_t(16) * 3 * sm_count() ? 1 :
 Schedule schedule_for(int nl, size_t tiles) {
     if (g_force) return *g_force;
     Schedule sc = size_class(tiles) ? Schedule{32, 0} : Schedule{0, 2};
-    if (g_tune.valid) sc = g_tune.s[layer_class(nl)][size_class(tiles)];
+    if (g_tune.set[layer_class(nl)][size_class(tiles)]) sc = g_tune.s[layer_class(nl)][size_class(tiles)];
     if (g_band_user >= 0) sc.band = g_band_user;
     return sc;
 }
@@ -1757,6 +1757,7 @@ extern "C" int32_t pcbg_autotune(void* stream, pcbg_tune_entry* out, int32_t cap
                 }
             cudaFree(buf);
             T.s[lc][sc] = best;
+            T.set[lc][sc] = true;
             T.ms[lc][sc] = best_ms;
             T.ms_untuned[lc][sc] = untuned_ms;
             if (out && written < cap) {
@@ -1767,7 +1768,59 @@ extern "C" int32_t pcbg_autotune(void* stream, pcbg_tune_entry* out, int32_t cap
                 e.searches = n; e.rw = rw; e.rh = rh; e.nl = nl;
             }
         }
-    T.valid = true;
     g_tune = T;
     return written;
+}
+
+// Tune on the caller's own batch: every schedule is timed on it (the fastest of two launches each), and the best
+// becomes the schedule of its class (its largest layer count, and whether it holds at least 16 tiles per resident
+// block). For a caller whose batches repeat in shape, such as the microbenchmark's waves.
+extern "C" int32_t pcbg_autotune_batch(pcbg_search* s, int32_t n, void* stream, pcbg_tune_entry* out) {
+    using namespace pcbg;
+    if (n <= 0) return 0;
+    std::vector<BatchItem> items(n);
+    int nlmax = 1;
+    size_t tiles = 0;
+    for (int k = 0; k < n; ++k) {
+        BatchItem& b = items[k];
+        const pcbg_search& q = s[k];
+        memset(&b, 0, sizeof(b));
+        b.rw = q.rw; b.rh = q.rh; b.nl = q.nl; b.pitch = q.pitch; b.hpad = q.hpad;
+        memcpy(b.fac, q.fac, sizeof(b.fac));
+        b.cf = q.cf; b.fl = q.flags; b.vcf = q.vcf;
+        b.start_idx = q.start_idx; b.start_d = q.start_d; b.n_starts = q.n_starts;
+        b.out = q.out;
+        nlmax = std::max(nlmax, q.nl);
+        tiles += size_t(q.pitch / TILE) * (q.hpad / TILE);
+    }
+    std::lock_guard<std::mutex> g(g_mu);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int bands[] = {0, 8, 16, 32, 64, 128};
+    float best_ms = 1e30f, untuned_ms = 1e30f;
+    Schedule best{DEFAULT_BAND, 0};
+    for (int band : bands)
+        for (int minb = 2; minb <= 3; ++minb) {
+            const Schedule cand{band, minb};
+            g_force = &cand;
+            float ms = 1e30f;
+            for (int rep = 0; rep < 2; ++rep) {
+                if (solve_batch_locked(items.data(), n, st) != 0) { g_force = nullptr; return PCBG_ERR_FAIL; }
+                ms = std::min(ms, t_stats.kernel_ms);
+            }
+            g_force = nullptr;
+            if (ms < best_ms) { best_ms = ms; best = cand; }
+            if (band == DEFAULT_BAND && minb == 3) untuned_ms = ms;
+        }
+    const int lc = layer_class(nlmax), sc = size_class(tiles);
+    g_tune.s[lc][sc] = best;
+    g_tune.set[lc][sc] = true;
+    g_tune.ms[lc][sc] = best_ms;
+    g_tune.ms_untuned[lc][sc] = untuned_ms;
+    if (out) {
+        out->layers_lo = 2 * lc + 1; out->layers_hi = 2 * lc + 2; out->batch_class = sc;
+        out->band = best.band; out->blocks_per_sm = best.minb;
+        out->ms = best_ms; out->ms_untuned = untuned_ms;
+        out->searches = n; out->rw = 0; out->rh = 0; out->nl = nlmax;
+    }
+    return 1;
 }
