@@ -464,3 +464,21 @@ def test_round_cap_stops_the_launch_and_the_device_stays_usable(gpu):
     assert arr[0].best == best
     got = s["out"].cpu().numpy().reshape(s["nl"], s["rh"], s["rw"])
     assert np.array_equal(got.view(np.uint32), field.view(np.uint32))
+
+
+def test_autotuned_schedule_keeps_results(gpu):
+    """pcbg_autotune_batch times every schedule on a batch and keeps the fastest for its class; the solves that then
+    take the tuned schedule still give the oracle's fields."""
+    lib = _lib.load()
+    searches = [make_device_search(9950 + k, 300 + 40 * k, 260, 2 + k % 5, 14.0) for k in range(6)]
+    arr = run_batch(searches)
+    e = _lib.TuneEntry()
+    assert lib.pcbg_autotune_batch(arr, len(searches), None, C.byref(e)) == 1, _lib.last_error()
+    assert e.band in (0, 8, 16, 32, 64, 128) and e.blocks_per_sm in (2, 3) and e.ms > 0
+    arr = run_batch(searches)
+    assert lib.pcbg_round_band() == e.band
+    for k, s in enumerate(searches):
+        field, best, bd = oracle_of(s)
+        assert arr[k].best == best
+        got = s["out"].cpu().numpy().reshape(s["nl"], s["rh"], s["rw"])
+        assert np.array_equal(got.view(np.uint32), field.view(np.uint32)), k
