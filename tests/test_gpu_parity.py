@@ -185,13 +185,12 @@ def test_round_band_changes_work_not_results(gpu, band):
     for k in range(10):
         rw, rh = int(rng.integers(60, 700)), int(rng.integers(60, 700))
         searches.append(make_device_search(9700 + k, rw, rh, int(rng.integers(2, 7)), float(rng.integers(8, 33))))
-    old = lib.pcbg_round_band()
     lib.pcbg_set_round_band(band)
     try:
         arr = run_batch(searches)
         deferred = lib.pcbg_last_batch_deferred()
     finally:
-        lib.pcbg_set_round_band(old)
+        lib.pcbg_set_round_band(-1)   # back to the tuned / default band
     if band == 0:
         assert deferred == 0
     for k, s in enumerate(searches):
