@@ -675,10 +675,14 @@ __device__ void visit_tile(const SolveArgs& a, int s, int tile, int round, unsig
         sh.marks = 0; sh.any = 0; sh.wide = 0; sh.iters = 0; sh.tmin = ~0ull; sh.wmax = 0;
         sh.wcnt = 0; sh.wsum = 0;
         for (int b = 0; b < 8; ++b) sh.mkey[b] = KEY_NONE;
-        // which halo sides changed since the last visit, and the key that queued the tile; taken before the halo
-        // is read, so a neighbour that marks us afterwards has also queued us for the next round with its key
-        sh.sides = atomicExch(S.sides + tile, 0u);
+        // The key that queued the tile and which halo sides changed since the last visit, taken before the halo is
+        // read, so that a neighbour that marks us afterwards has also queued us for the next round with its key.
+        // The key goes first: a marking neighbour sets its side bit before it lowers the key (with a fence between),
+        // so a visit that takes a mark's key also takes that mark's side bit, and a round that finds the key gone
+        // may skip the tile (its marks were all consumed by a visit that walked their sides).
         sh.kvis = a.ordered ? atomicExch(S.tkey + tile, KEY_NONE) : KEY_NONE;
+        __threadfence();
+        sh.sides = atomicExch(S.sides + tile, 0u);
         __threadfence();   // the halo reads below come after the exchange that saw the neighbours' marks
     }
     __syncthreads();
@@ -887,11 +891,13 @@ __device__ void visit_tile(const SolveArgs& a, int s, int tile, int round, unsig
         const int nx = tx + DXs[b], ny = ty + DYs[b];
         if (nx >= 0 && ny >= 0 && nx < S.ntx && ny < S.nty) {
             atomicOr(S.sides + ny * S.ntx + nx, opposite_side(b));   // the side of the neighbour facing us
+            __threadfence();                                           // the side bit before the key (see above)
             queue_tile(a, S, s, ny * S.ntx + nx, round + 1, sh.mkey[b]);
         }
     }
     if (tid == 8 && requeue) {
         atomicOr(S.sides + tile, SIDE_ALL);
+        __threadfence();
         queue_tile(a, S, s, tile, round + 1, sh.kvis == KEY_NONE ? 0u : sh.kvis);
     }
     __syncthreads();
