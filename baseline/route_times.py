@@ -43,8 +43,11 @@ def run(binary, dsn, args, timeout, env=None):
     e.update(env or {})
     with tempfile.TemporaryDirectory() as d:
         ses = os.path.join(d, "b.ses")
-        r = subprocess.run([os.path.join(BIN, binary), "-de", dsn, "-do", ses, "-v", *args], capture_output=True,
-                           text=True, timeout=timeout, env=e)
+        try:
+            r = subprocess.run([os.path.join(BIN, binary), "-de", dsn, "-do", ses, "-v", *args], capture_output=True,
+                               text=True, timeout=timeout, env=e)
+        except subprocess.TimeoutExpired:
+            return {"rc": None, "route_s": None, "timeout_s": timeout}
         data = open(ses, "rb").read() if os.path.exists(ses) else b""
         ev = subprocess.run([os.path.join(BIN, binary), "-de", dsn, "--eval", ses], capture_output=True, text=True,
                             timeout=timeout, env=e).stdout.strip() if data else ""
