@@ -302,6 +302,8 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="skip the schedule autotuner (untuned rule)")
     ap.add_argument("--band", type=int, default=None,
                     help="relaxation round band (pcbg_set_round_band); default: the library's own")
+    ap.add_argument("--order", type=int, default=None, choices=[0, 1, 2],
+                    help="visit order of ordered rounds (pcbg_set_visit_order); default: the library's own")
     ap.add_argument("--cost-maps-only", type=int, nargs=2, metavar=("NX", "NY"), default=None,
                     help="only time the cost-map rebuild on an NX x NY x 8 board of 4 classes (a profiling case)")
     args = ap.parse_args()
@@ -321,6 +323,8 @@ def main():
     lib = _lib.load()
     if args.band is not None:
         lib.pcbg_set_round_band(args.band)
+    if args.order is not None:
+        lib.pcbg_set_visit_order(args.order)
     if args.cost_maps_only:
         if rank == 0:
             print(json.dumps(cost_map_roofline(lib, peaks()[0], *args.cost_maps_only)))
@@ -432,6 +436,7 @@ def main():
     states = [sum(s["rw"] * s["rh"] * s["nl"] for s in w) for w in dev_waves]
 
     iters = [0, 0, 0, 0]
+    busy = [0.0]
 
     def solve(k):
         arr, _ = arrays[k % len(arrays)]
@@ -442,6 +447,7 @@ def main():
         iters[1] += lib.pcbg_last_batch_deferred()
         iters[2] += lib.pcbg_last_batch_dropped()
         iters[3] += lib.pcbg_last_batch_settled()
+        busy[0] += lib.pcbg_last_batch_busy_frac() * lib.pcbg_last_batch_kernel_ms()
         return (lib.pcbg_last_batch_kernel_ms(), lib.pcbg_last_batch_tile_visits(), lib.pcbg_last_batch_layer_visits(),
                 lib.pcbg_last_batch_launches(), lib.pcbg_last_batch_rounds())
 
@@ -457,6 +463,7 @@ def main():
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     kms, tv, lv, launches, rounds, st_done = 0.0, 0, 0, 0, 0, 0
     iters[:] = [0, 0, 0, 0]
+    busy[0] = 0.0
     with ClockSampler(local) as clk:
         e0.record(stream)
         for k in range(args.steps):
@@ -614,6 +621,8 @@ def main():
                              "local_iters_per_visit": round(iters[0] / max(1, tv), 3),
                              "round_band": int(lib.pcbg_round_band()),
                              "blocks_per_sm": int(lib.pcbg_last_batch_blocks_per_sm()),
+                             "visit_order": int(lib.pcbg_visit_order()),
+                             "block_time_visiting": round(busy[0] / max(kms, 1e-9), 4),
                              "autotuned_schedules": tune,
                              "tiles_deferred_per_step": iters[1] // args.steps,
                              "tiles_dropped_per_step": iters[2] // args.steps},

@@ -164,6 +164,14 @@ int64_t pcbg_last_batch_dropped(void);
 /* States the last batch reported: at or below each search's best target's cost (every reached state of a search
  * that reached no target). */
 int64_t pcbg_last_batch_settled(void);
+/* Share of the relaxation launches' block time spent visiting tiles (SM cycles, summed over blocks); the rest is the
+ * round filters and the waits at grid barriers for a round's last visits. */
+float pcbg_last_batch_busy_frac(void);
+/* Order in which an ordered round's visits are taken: 0 as listed, 1 the lower half of each search's band first,
+ * 2 the tiles of the searches with the most layers first (a value outside 0-2 selects it). Results are the same for
+ * every order. Default 2, or PCBG_VISIT_ORDER from the environment. */
+void pcbg_set_visit_order(int32_t order);
+int32_t pcbg_visit_order(void);
 
 /* Scheduling of the relaxation rounds (no reference counterpart; the reference sweeps whole windows, src/gpu.cu:
  * 493-524). A queued tile carries the least distance among the edge improvements that queued it; with band B > 0 a

@@ -27,7 +27,7 @@ PCBG_SYMBOLS = [
     "pcbg_mirror_history", "pcbg_mirror_download", "pcbg_sched_add_log_host", "pcbg_rsched_mode",
     "pcbg_rsched_begin", "pcbg_rsched_net", "pcbg_rsched_allow", "pcbg_rsched_started", "pcbg_rsched_committed",
     "pcbg_rsched_verdict", "pcbg_rsched_end", "pcbg_rsched_get_stats", "pcbg_autotune", "pcbg_autotune_batch",
-    "pcbg_last_batch_blocks_per_sm",
+    "pcbg_last_batch_blocks_per_sm", "pcbg_last_batch_busy_frac", "pcbg_set_visit_order", "pcbg_visit_order",
     "pcbg_synth_search_host", "pcbg_costs_create", "pcbg_costs_destroy", "pcbg_costs_set_static",
     "pcbg_costs_set_occupancy", "pcbg_costs_set_history", "pcbg_costs_set_ground", "pcbg_costs_rebuild",
     "pcbg_costs_stamp", "pcbg_costs_add_history", "pcbg_costs_download", "pcbg_costs_download_history",
@@ -164,6 +164,10 @@ def load() -> C.CDLL:
     lib.pcbg_autotune_batch.argtypes = [C.POINTER(Search), C.c_int32, C.c_void_p, C.c_void_p]
     lib.pcbg_autotune_batch.restype = C.c_int32
     lib.pcbg_last_batch_blocks_per_sm.restype = C.c_int32
+    lib.pcbg_last_batch_busy_frac.restype = C.c_float
+    lib.pcbg_set_visit_order.argtypes = [C.c_int32]
+    lib.pcbg_set_visit_order.restype = None
+    lib.pcbg_visit_order.restype = C.c_int32
     lib.pcbg_set_round_band.argtypes = [C.c_int32]
     lib.pcbg_set_round_band.restype = None
     lib.pcbg_round_band.restype = C.c_int32

@@ -97,6 +97,8 @@ struct BatchStats {
     long long deferred = 0;        // ordered rounds: tiles listed for a round and passed on to the next one
     long long dropped = 0;         // ordered rounds: tiles dropped because nothing that queued them can matter
     long long settled = 0;         // states at or below their search's best target's cost (all reached when none)
+    long long busy_cycles = 0;     // relaxation launches: SM cycles the blocks spent visiting tiles, summed
+    long long block_cycles = 0;    // and the SM cycles they were resident (visiting, filtering, at grid barriers)
     int band = 0;                  // round band of the (last) relaxation launch
     int blocks_per_sm = 0;         // resident blocks per SM of its build
 };

@@ -54,14 +54,18 @@ constexpr long long BAR_SPIN_LIMIT = 1ll << 24;   // polls (with __nanosleep) be
 constexpr uint32_t KEY_NONE = 0xFFFFFFFFu;   // tile key / round minimum: nothing queued
 
 // control words of a batch: per rotating round the queued count and the next item taken; per round parity the
-// count and next item of the round's visit list (ordered rounds)
+// counts of the round's visit list filled from its front and from its back, and the next item taken (ordered rounds)
 // (C_WIDEN: the doublings of the band the next ordered round uses)
 enum { C_CNT = 0, C_NEXT = 3, C_BAR = 6, C_GEN = 7, C_ERR = 8, C_ROUNDS = 9, C_VCNT = 10, C_VNEXT = 12, C_WIDEN = 14,
-       C_N = 16 };
+       C_BCNT = 16, C_N = 18 };
 constexpr unsigned int MAX_WIDEN = 12;   // band x 4096: wider than any search's key range, i.e. unordered
 enum { ERR_BARRIER = 1, ERR_ROUNDS = 2, ERR_OVERFLOW = 4 };
-// counters of a launch: tile visits, layer visits, local iterations, tiles deferred to a later round, tiles dropped
-constexpr int NVIS = 5;
+// counters of a launch: tile visits, layer visits, local iterations, tiles deferred to a later round, tiles dropped,
+// SM cycles the blocks spent visiting tiles, SM cycles the blocks were resident (both summed over blocks)
+constexpr int NVIS = 7;
+// order of an ordered round's visit list: 0 as filtered, 1 the lower half of each search's band first, 2 the tiles
+// of the searches with the most layers first
+enum { ORDER_FIFO = 0, ORDER_KEY = 1, ORDER_LAYERS = 2 };
 
 template <typename DT> struct Lim;
 template <> struct Lim<uint32_t> {
@@ -103,6 +107,7 @@ struct SolveArgs {
     int max_rounds;
     int ordered;                  // 1: rounds in distance bands (32-bit distances only), 0: every queued tile
     unsigned int band;            // band width of an ordered round, in multiples of the search's weight scale
+    int order;                    // ORDER_*: which visits of an ordered round go to the front of its list
 };
 
 // Key of an improvement: its distance, as 32 bits (64-bit distances run unordered and only need "some key").
@@ -904,14 +909,16 @@ __device__ void visit_tile(const SolveArgs& a, int s, int tile, int round, unsig
 }
 
 // Two builds of the kernel: MINB = 2 blocks per SM with up to 80 registers a thread, or MINB = 3 within 56
-// registers (the 32-bit build spills 80 bytes). A third resident block fills more of the time that warps wait at the
+// registers (the 32-bit build spills 124 bytes). A third resident block fills more of the time that warps wait at the
 // local-iteration barrier, but each block runs slower; relax_launch takes it only for batches with many tiles.
 template <typename DT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) relax_kernel(SolveArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ unsigned int sh_item_hi, sh_item_lo, sh_stop;
+    __shared__ long long sh_t0, sh_tv, sh_busy;   // SM clock at start and at the current visit; cycles visiting
     const unsigned int nblocks = gridDim.x;
     const int tid = threadIdx.x;
+    if (tid == 0) { sh_t0 = clock64(); sh_busy = 0; }
     int round = 1;
     for (;; ++round) {
         const int buf = round % 3;
@@ -921,7 +928,7 @@ __global__ void __launch_bounds__(NT, MINB) relax_kernel(SolveArgs a) {
         // rounds) the visit list that the filter below builds from it.
         const unsigned long long* items = a.wl + size_t(buf) * a.cap;
         unsigned int* next = a.ctl + C_NEXT + buf;
-        unsigned int vcnt = cnt;
+        unsigned int vcnt = cnt, vfront = cnt;
         if (a.ordered) {
             // Filter, all threads of the grid over the round's list. A tile whose key is gone was visited after it
             // was listed (its improvements with it); one keyed above the search's best target has nothing that
@@ -930,7 +937,11 @@ __global__ void __launch_bounds__(NT, MINB) relax_kernel(SolveArgs a) {
             const int vp = round & 1;
             const unsigned int widen = *reinterpret_cast<volatile unsigned int*>(a.ctl + C_WIDEN);
             const unsigned long long band = static_cast<unsigned long long>(a.band) << widen;
-            if (blockIdx.x == 0 && tid == 0) { a.ctl[C_VCNT + (vp ^ 1)] = 0; a.ctl[C_VNEXT + (vp ^ 1)] = 0; }
+            if (blockIdx.x == 0 && tid == 0) {
+                a.ctl[C_VCNT + (vp ^ 1)] = 0;
+                a.ctl[C_BCNT + (vp ^ 1)] = 0;
+                a.ctl[C_VNEXT + (vp ^ 1)] = 0;
+            }
             for (int q = blockIdx.x * NT + tid; q < a.n; q += nblocks * NT) a.st[q].kmin[(round + 2) % 3] = KEY_NONE;
             unsigned int deferred = 0, dropped = 0;
             for (unsigned int k = blockIdx.x * NT + tid; k < cnt; k += nblocks * NT) {
@@ -951,8 +962,21 @@ __global__ void __launch_bounds__(NT, MINB) relax_kernel(SolveArgs a) {
                     ++deferred;
                     continue;
                 }
-                const unsigned int pos = atomicAdd(a.ctl + C_VCNT + vp, 1u);
-                a.vl[pos] = it;
+                // Front or back of the visit list; blocks take the front first, then the back from its end. Each
+                // listed item is placed at most once, so the two parts (at most cnt <= cap items) never meet.
+                bool front = true;
+                if (a.order == ORDER_KEY)
+                    front = thr == ~0ull || key <= km ||
+                            2ull * (key - km) <= static_cast<unsigned long long>(ws) * band;
+                else if (a.order == ORDER_LAYERS)
+                    front = 2 * S.nl > a.nlmax;
+                if (front) {
+                    const unsigned int pos = atomicAdd(a.ctl + C_VCNT + vp, 1u);
+                    a.vl[pos] = it;
+                } else {
+                    const unsigned int pos = atomicAdd(a.ctl + C_BCNT + vp, 1u);
+                    a.vl[a.cap - 1u - pos] = it;
+                }
             }
             deferred = __reduce_add_sync(0xFFFFFFFFu, deferred);
             dropped = __reduce_add_sync(0xFFFFFFFFu, dropped);
@@ -961,7 +985,8 @@ __global__ void __launch_bounds__(NT, MINB) relax_kernel(SolveArgs a) {
             grid_barrier(a.ctl, nblocks);
             items = a.vl;
             next = a.ctl + C_VNEXT + vp;
-            vcnt = *reinterpret_cast<volatile unsigned int*>(a.ctl + C_VCNT + vp);
+            vfront = *reinterpret_cast<volatile unsigned int*>(a.ctl + C_VCNT + vp);
+            vcnt = vfront + *reinterpret_cast<volatile unsigned int*>(a.ctl + C_BCNT + vp);
             // A round whose visit list cannot keep every block busy widens the next round's band (doubling it, up
             // to unordered); a round with far more tiles than blocks narrows it again. Read by every block only
             // after the end-of-round barrier, so the whole grid uses one band per round.
@@ -976,7 +1001,8 @@ __global__ void __launch_bounds__(NT, MINB) relax_kernel(SolveArgs a) {
             if (tid == 0) {
                 const unsigned int k = atomicAdd(next, 1u);
                 if (k < vcnt) {
-                    const unsigned long long it = __ldcg(items + k);   // written last round, or by the filter
+                    // written last round, or by the filter (the back part from the list's end)
+                    const unsigned long long it = __ldcg(items + (k < vfront ? k : a.cap - 1u - (k - vfront)));
                     sh_item_hi = unsigned(it >> 32);
                     sh_item_lo = unsigned(it & 0xFFFFFFFFu);
                 } else {
@@ -987,7 +1013,9 @@ __global__ void __launch_bounds__(NT, MINB) relax_kernel(SolveArgs a) {
             const unsigned int hi = sh_item_hi, lo = sh_item_lo;
             __syncthreads();
             if (hi == 0xFFFFFFFFu) break;
-            visit_tile<DT>(a, int(hi), int(lo), round, smem);
+            if (tid == 0) sh_tv = clock64();
+            visit_tile<DT>(a, int(hi), int(lo), round, smem);   // ends with a block barrier
+            if (tid == 0) sh_busy += clock64() - sh_tv;
         }
         // the list consumed last round is free: clear it for the round after next
         if (blockIdx.x == 0 && tid == 0) {
@@ -1009,6 +1037,10 @@ __global__ void __launch_bounds__(NT, MINB) relax_kernel(SolveArgs a) {
         if (sh_stop) break;
     }
     if (blockIdx.x == 0 && tid == 0) a.ctl[C_ROUNDS] = unsigned(round);
+    if (tid == 0) {
+        atomicAdd(a.visits + 5, static_cast<unsigned long long>(sh_busy));
+        atomicAdd(a.visits + 6, static_cast<unsigned long long>(clock64() - sh_t0));
+    }
 }
 
 // starts: distance init (least per state) and the first round's tiles. A start's value is written here, not by a
@@ -1165,6 +1197,16 @@ int max_rounds_from_env() {
     return v >= 1 ? v : (1 << 20);
 }
 int g_max_rounds = max_rounds_from_env();
+
+// Order of an ordered round's visit list (ORDER_*): pcbg_set_visit_order, or PCBG_VISIT_ORDER in the environment.
+// Default: the searches with the most layers first. Their visits take longest, and a round ends when its last visit
+// does, so taking them first leaves the short visits to fill the end of the round (longest-first list scheduling).
+int visit_order_from_env() {
+    const char* e = std::getenv("PCBG_VISIT_ORDER");
+    const int v = e ? std::atoi(e) : -1;
+    return v >= ORDER_FIFO && v <= ORDER_LAYERS ? v : ORDER_LAYERS;
+}
+int g_order = visit_order_from_env();
 
 thread_local std::string t_err;
 thread_local BatchStats t_stats;
@@ -1328,7 +1370,7 @@ int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream
     // from pageable memory would go through the driver's bounce buffer one call at a time)
     const size_t h_sd = 0, h_st = round_up(sizeof(SDev) * m, 16), h_sp = h_st + round_up(sizeof(SStat) * m, 16);
     const size_t h_res = h_sp + round_up(size_t(m) * 20, 16), h_ctl = h_res + round_up(sizeof(SStat) * m, 16);
-    const size_t h_vis = h_ctl + 64, h_end = h_vis + NVIS * 8;
+    const size_t h_vis = h_ctl + round_up(C_N * 4, 16), h_end = h_vis + NVIS * 8;
     if (!host_stage(h_end)) { t_err = "pinned allocation failed"; return -1; }
     unsigned char* hs = g_hstage.p;
     memcpy(hs + h_sd, sd.data(), sizeof(SDev) * m);
@@ -1368,6 +1410,7 @@ int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream
     a.max_rounds = g_max_rounds;
     a.band = unsigned(band);
     a.ordered = band > 0 ? 1 : 0;
+    a.order = g_order;
     seed_kernel<DT><<<m, 128, 0, stream>>>(a, d_sip, d_sdp, d_ns);
     const RelaxLaunch R = relax_launch<DT>(smem, tiles, sc.minb);
     bs.band = band;
@@ -1408,6 +1451,8 @@ int run_batch(BatchItem* items, const std::vector<int>& idx, cudaStream_t stream
     bs.local_iters += (long long)visits[2];
     bs.deferred += (long long)visits[3];
     bs.dropped += (long long)visits[4];
+    bs.busy_cycles += (long long)visits[5];
+    bs.block_cycles += (long long)visits[6];
     const int rounds_out = int(ctl[C_ROUNDS]);
     const unsigned long long INF = static_cast<unsigned long long>(Lim<DT>::INF);
     for (int k = 0; k < m; ++k) {
@@ -1502,6 +1547,18 @@ extern "C" int64_t pcbg_last_batch_local_iters(void) { return pcbg::last_stats()
 extern "C" int64_t pcbg_last_batch_deferred(void) { return pcbg::last_stats().deferred; }
 extern "C" int64_t pcbg_last_batch_dropped(void) { return pcbg::last_stats().dropped; }
 extern "C" int64_t pcbg_last_batch_settled(void) { return pcbg::last_stats().settled; }
+extern "C" float pcbg_last_batch_busy_frac(void) {
+    const pcbg::BatchStats& b = pcbg::last_stats();
+    return b.block_cycles > 0 ? float(double(b.busy_cycles) / double(b.block_cycles)) : 0.f;
+}
+extern "C" void pcbg_set_visit_order(int32_t order) {
+    std::lock_guard<std::mutex> g(pcbg::g_mu);
+    pcbg::g_order = order >= pcbg::ORDER_FIFO && order <= pcbg::ORDER_LAYERS ? order : pcbg::ORDER_LAYERS;
+}
+extern "C" int32_t pcbg_visit_order(void) {
+    std::lock_guard<std::mutex> g(pcbg::g_mu);
+    return pcbg::g_order;
+}
 
 extern "C" void pcbg_set_round_band(int32_t band) {
     std::lock_guard<std::mutex> g(pcbg::g_mu);
@@ -1538,7 +1595,7 @@ constexpr size_t NA_WL = NA_TKEY + NA_TILES * 4;
 constexpr size_t NA_VL = NA_WL + NA_TILES * 3 * 8;
 constexpr size_t NA_SMALL = NA_VL + NA_TILES * 8;
 // offsets in the small area after the lists
-constexpr size_t NA_SDEV = 0, NA_SSTAT = 1024, NA_CTL = 1088, NA_VIS = 1152, NA_SPTR = 1216;
+constexpr size_t NA_SDEV = 0, NA_SSTAT = 1024, NA_CTL = 1088, NA_VIS = 1168, NA_SPTR = 1232;
 static_assert(sizeof(SDev) <= NA_SSTAT - NA_SDEV && sizeof(SStat) <= NA_CTL - NA_SSTAT &&
               C_N * 4 <= NA_VIS - NA_CTL && NVIS * 8 <= NA_SPTR - NA_VIS && NA_SPTR + 24 <= 4096,
               "no-alloc small area layout");
@@ -1624,6 +1681,7 @@ int na_run(pcbg_search* q, unsigned char* base, cudaStream_t stream, int band, i
     a.max_rounds = g_max_rounds;
     a.band = unsigned(band);
     a.ordered = sizeof(DT) == 4 && band > 0 ? 1 : 0;
+    a.order = g_order;
     const uint32_t* const* sip = reinterpret_cast<const uint32_t* const*>(small + NA_SPTR);
     const uint64_t* const* sdp = reinterpret_cast<const uint64_t* const*>(small + NA_SPTR + 8);
     const int* nsp = reinterpret_cast<const int*>(small + NA_SPTR + 16);

@@ -202,6 +202,33 @@ def test_round_band_changes_work_not_results(gpu, band):
         assert np.array_equal(got.view(np.uint32), field.view(np.uint32)), (band, k)
 
 
+@pytest.mark.parametrize("order", [0, 1, 2])
+def test_visit_order_changes_work_not_results(gpu, order):
+    """The order of an ordered round's visits (pcbg_set_visit_order: as listed, the lower half of each search's band
+    first, the searches with the most layers first) changes which visits see which neighbours' results, never the
+    fixed point. The visit list's two-ended filling is checked with a narrow band (many deferred tiles, rounds of
+    both parts) on searches of 2 to 6 layers; the busy share is a fraction."""
+    lib = _lib.load()
+    rng = np.random.default_rng(78)
+    searches = []
+    for k in range(12):
+        rw, rh = int(rng.integers(100, 900)), int(rng.integers(100, 900))
+        searches.append(make_device_search(9600 + k, rw, rh, int(rng.integers(2, 7)), float(rng.integers(8, 33))))
+    prev = lib.pcbg_visit_order()
+    lib.pcbg_set_round_band(4)
+    lib.pcbg_set_visit_order(order)
+    try:
+        assert lib.pcbg_visit_order() == order
+        arr = run_batch(searches)
+        busy = lib.pcbg_last_batch_busy_frac()
+        assert lib.pcbg_last_batch_deferred() > 0
+    finally:
+        lib.pcbg_set_round_band(-1)
+        lib.pcbg_set_visit_order(prev)
+    assert 0.0 < busy <= 1.0, busy
+    _check_fields(searches, arr, _oracle_many(searches), f"order {order}")
+
+
 def test_walkback_matches_oracle(gpu):
     """The device walk-back (one warp per search, after the relaxation) equals the oracle's walk over its exact
     field: the same states in the same order, best target first, ending on the start."""
