@@ -45,7 +45,7 @@ BYTES_PER_STATE_VISIT = 12
 # DRAM bytes moved per algorithmic byte by relax_kernel, from one ncu capture of the 64-search case
 # (dram__bytes_read.sum + dram__bytes_write.sum over 12 B per state visit). A full wave is too large to capture; its
 # traffic grows with the state visits, so the bench scales this ratio by the launch's algorithmic bytes.
-NCU_TRAFFIC_PER_ALG_BYTE = 0.34
+NCU_TRAFFIC_PER_ALG_BYTE = 0.93
 
 
 def peaks():
