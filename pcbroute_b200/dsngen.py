@@ -119,8 +119,8 @@ CONFIGS = {
                  (3, 6), [("default", 150, 150, 0.6), ("signal", 200, 150, 0.2), ("power", 400, 250, 0.15),
                           ("hv", 500, 400, 0.05)], [("GND", "In1.Cu"), ("VCC", "In6.Cu")]),
     # small boards for the parity tests
-    "t1": Config("t1", 24, 18, ["F.Cu", "B.Cu"], [("SOIC8", 3), ("R0805", 4)], 10, 14),
-    "t2": Config("t2", 30, 24, ["F.Cu", "In1.Cu", "In2.Cu", "B.Cu"], [("SOIC8", 4), ("R0603", 6)], 16, 24, 0.2, (3, 4),
+    "t1": Config("t1", 24, 18, ["F.Cu", "B.Cu"], [("SOIC8", 3), ("R0805", 4)], 10, 10),
+    "t2": Config("t2", 30, 24, ["F.Cu", "In1.Cu", "In2.Cu", "B.Cu"], [("SOIC8", 4), ("R0603", 6)], 16, 22, 0.2, (3, 4),
                  [("default", 200, 150, 0.8), ("power", 400, 250, 0.2)]),
 }
 
