@@ -178,7 +178,8 @@ int32_t pcbg_visit_order(void);
  * round of a search visits only the tiles keyed within B weight scales of the least key queued for it (the weight
  * scale: the mean straight-move weight of the search's cheapest well-filled tile), defers the rest to a later round
  * and drops tiles keyed above the best target found. B = 0 visits every queued tile each round. Results are the
- * same for every B; only the work changes. Default 16. */
+ * same for every B; only the work changes. Default (a value < 0): the autotuned band of the batch's class, or before
+ * any tuning 0 for batches of fewer than 16 tiles per resident block and 32 for larger ones. */
 void pcbg_set_round_band(int32_t band);
 int32_t pcbg_round_band(void);     /* the band of the last batch solved on this thread */
 /* The schedule autotuner: for each layer-count class (1-2, 3-4, 5-6, 7-8 layers) and batch class (0: fewer than 16
