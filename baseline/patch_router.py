@@ -4,11 +4,16 @@
 
 A build recipe: it reads the router's source where it lies and writes the patched copy under baseline/_ref/ (git-
 ignored); nothing of the router's source enters this repository. Each hook goes in at one site, found by a short
-fragment of the line it follows or extends; the script stops with an error if a fragment is not found exactly once
-in its function, so a changed router fails to build instead of building without a hook. The hooks read the
-router's state and change none of it (see router_hooks.h).
+fragment of the line it follows or extends: the first occurrence after the opening line of the function that holds
+the site (the worker's wait condition must occur exactly once in the file). The script stops with an error if a
+site is not found, or if the result does not hold each of the eight hook calls exactly once, so a changed router
+fails to build instead of building without a hook. The hooks read the router's state and change none of it (see
+router_hooks.h).
 """
 import sys
+
+HOOKS = ("pcbgh_rebuilt", "pcbgh_refreshed", "pcbgh_begin", "pcbgh_allow", "pcbgh_started", "pcbgh_verdict",
+         "pcbgh_commit", "pcbgh_end")
 
 
 def insert_after(src, scope, anchor, text, start=0):
@@ -21,9 +26,8 @@ def insert_after(src, scope, anchor, text, start=0):
     return src[:k] + text + src[k:]
 
 
-def main():
-    src_path, out_path = sys.argv[1], sys.argv[2]
-    s = open(src_path).read()
+def patch(s):
+    """The router source `s` with the hook calls added."""
     # mirror: every grid after a rebuild, the changed spans after a refresh
     s = insert_after(s, "void rebuild_costs(float pres, bool hard) {", "for (auto& t : th) t.join();\n",
                      "        pcbgh_rebuilt(rcs, hist, NL, G.nx, G.ny);\n")
@@ -49,6 +53,15 @@ def main():
     s = insert_after(s, rw, "commits.push_back(std::move(blocks));\n",
                      "                            pcbgh_commit(cursor, commits.size() - 1);\n")
     s = insert_after(s, rw, "for (auto& t : th) t.join();\n", "            pcbgh_end();\n")
+    for h in HOOKS:
+        if s.count(h + "(") != 1:
+            raise SystemExit(f"patch_router: {h} is not called exactly once in the patched router")
+    return s
+
+
+def main():
+    src_path, out_path = sys.argv[1], sys.argv[2]
+    s = patch(open(src_path).read())
     with open(out_path, "w") as f:
         f.write(s)
 
