@@ -494,24 +494,32 @@ void rs_init() {
     if (!m) return;
     const std::string mode(m);
     if (const char* t = std::getenv("PCBG_SCHED_THRESHOLD")) g_rs.threshold = float(std::atof(t));
+    // a scheduler asked for but not usable leaves the router's own speculation, and says so once
+    auto off = [](const char* why, const char* what) {
+        std::fprintf(stderr, "pcbg: PCBG_SCHED=%s: %s; speculation stays the router's own\n", what, why);
+    };
     if (mode == "log") {
         const char* p = std::getenv("PCBG_SCHED_LOG");
-        if (!p) return;
+        if (!p) return off("PCBG_SCHED_LOG is not set", "log");
         g_rs.log_path = p;
         g_rs.S = pcbg_sched_create(1);
-        if (g_rs.S) g_rs.mode = 1;
+        if (!g_rs.S) return off("the predictor could not be created on the device", "log");
+        g_rs.mode = 1;
     } else if (mode == "learned") {
         const char* p = std::getenv("PCBG_SCHED_MODEL");
-        if (!p) return;
+        if (!p) return off("PCBG_SCHED_MODEL is not set", "learned");
         g_rs.S = pcbg_sched_create(1);
-        if (!g_rs.S) return;
+        if (!g_rs.S) return off("the predictor could not be created on the device", "learned");
         std::vector<float> w(g_rs.S->net.nparams);
         FILE* f = std::fopen(p, "rb");
-        if (!f) return;
+        if (!f) return off("the model file cannot be opened", "learned");
         const size_t got = std::fread(w.data(), 4, w.size(), f);
         std::fclose(f);
-        if (got != w.size() || pcbg_sched_set_params(g_rs.S, w.data()) != 0) return;
+        if (got != w.size()) return off("the model file holds fewer parameters than the predictor", "learned");
+        if (pcbg_sched_set_params(g_rs.S, w.data()) != 0) return off("the parameters could not be loaded", "learned");
         g_rs.mode = 2;
+    } else {
+        off("unknown mode (log or learned)", m);
     }
 }
 
