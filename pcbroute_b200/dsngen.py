@@ -63,6 +63,11 @@ def _bga256():
     return Footprint("BGA256", pads, 18000, 18000)
 
 
+# The SOIC padstack is 0.6 mm across the pad rows and 1.55 mm along them: transposed against the land pattern above
+# (1.55 mm across, 0.6 mm along), so the pads of adjacent SOIC-8 pins overlap by 0.28 mm. Every board this repository
+# has routed and timed was generated with it. Pins of one net whose pads touch make one piece, so the router counts
+# a connection fewer for each such pair (c1 seed 1: 55 of 56). Correcting it changes every board, and with them the
+# recorded route times and session digests, which were all taken on these boards.
 PADSTACKS = {
     "SOIC": ("rect", -300, -775, 300, 775),
     "C0805": ("rect", -500, -650, 500, 650),
