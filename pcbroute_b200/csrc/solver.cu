@@ -21,7 +21,9 @@
 //     the least improved edge distance that queued it, and a round visits only the tiles whose key lies within a
 //     band of the search's least key; the others wait for a later round, and tiles keyed above the search's best
 //     target are dropped. Tiles visited concurrently in one round read each other's old edges, so an unordered
-//     round revisits a tile each time a wave of improvements crosses it; the band keeps the visits near the front.
+//     round revisits a tile each time a wave of improvements crosses it; the band keeps the visits near the front;
+//   * within a round the visits of the searches with the most layers start first (they take longest, and a round
+//     ends with its last visit), so the short visits fill the end of the round.
 //
 // Exactness: distances are fixed-point integers (pcbg.h); min-plus over integers is exact and associative, so the
 // least fixed point is unique and any monotone schedule reaches it. A visit ends only after a full pass changed
