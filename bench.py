@@ -48,12 +48,20 @@ BYTES_PER_STATE_VISIT = 12
 NCU_TRAFFIC_PER_ALG_BYTE = 0.93
 
 
-def peaks():
-    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    if os.path.exists(p):
+def peaks(path=None):
+    """HBM copy bandwidth in GB/s and where it comes from: the measured figure of MEASURED_PEAKS.json (a number, or
+    an object with a burst / value figure), else the fallback copy bandwidth of 6650 GB/s."""
+    p = path or os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
         with open(p) as f:
-            d = json.load(f)
-        return float(d["hbm_gbs"]), "measured"
+            v = json.load(f).get("hbm_gbs")
+        if isinstance(v, dict):
+            v = v.get("burst", v.get("value"))
+        v = float(v)
+        if v > 0:
+            return v, "measured"
+    except (OSError, ValueError, TypeError, AttributeError):
+        pass
     return 6650.0, "fallback"
 
 

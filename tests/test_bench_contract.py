@@ -61,3 +61,17 @@ def test_reference_arm_under_two_ranks_prints_once():
     assert len(lines) == 1, r.stdout[-2000:]
     _check(lines[0], 1, 0)
     assert lines[0]["n_gpus"] == 2
+
+
+def test_peak_bandwidth_file_forms(tmp_path):
+    sys.path.insert(0, ROOT)
+    import bench
+    f = tmp_path / "peaks.json"
+    assert bench.peaks(str(tmp_path / "absent.json")) == (6650.0, "fallback")
+    f.write_text(json.dumps({"hbm_gbs": 6553.3, "bf16_tflops": 1590}))
+    assert bench.peaks(str(f)) == (6553.3, "measured")
+    f.write_text(json.dumps({"hbm_gbs": {"burst": 7001.5, "sustained": 6800}}))
+    assert bench.peaks(str(f)) == (7001.5, "measured")
+    for bad in ("{", json.dumps({"bf16_tflops": 1590}), json.dumps([1, 2]), json.dumps({"hbm_gbs": "n/a"})):
+        f.write_text(bad)
+        assert bench.peaks(str(f)) == (6650.0, "fallback"), bad
